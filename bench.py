@@ -1,0 +1,385 @@
+"""Benchmark: photons/s of the photon-tracking path on B200.
+
+One step = one full simulation of the workload (default: the layered tissue with a
+vessel, 256x256x128 voxels of 0.02 mm, uniform beam, 1e8 photons per GPU).
+
+  value  device throughput: photons / kernel time, inputs resident in HBM, timed
+         with CUDA events on the launching stream, L2 flushed between steps.
+  e2e    the same through the C ABI from pinned host buffers (mc3d_run: geometry,
+         optical table and safe-prime table uploaded, tallies read back each step),
+         timed on the host around the synchronous call.
+
+--impl reference runs the reference's own run_3dmc_gpu (compiled from its sources
+into oracle/_ref/gpu-mc-ref) on the same workload and GPU, on a bounded photon
+sample.  With torchrun (--gpus N) every rank runs one shard of a job of
+N x photons (disjoint RNG streams, weak scaling); the shards' integer tallies are
+summed over NCCL once per step, which is the path's only exchange.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+# Algorithmic operations per photon step, counted from the reference formulas
+# (src/mc3d_gpu.cu:181-339; each +, -, *, /, comparison, min, sqrt, rsqrt, log,
+# sin/cos counted once, integer and select operations not counted).  Of the 152,
+# 20 are special-function class (13 divisions, 2 sqrt, 2 rsqrt, 1 log, sin+cos of
+# sincospif); a Fresnel event (:226-257) adds 37, 6 of them special (acos, sin,
+# sqrt, 3 divisions).  The per-term breakdown is in DESIGN.md.
+OPS_STEP, SFU_STEP = 152, 20
+OPS_FRESNEL, SFU_FRESNEL = 37, 6
+FP32_LANES_PER_SM, SFU_LANES_PER_SM = 128, 16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--photons", type=float, default=1e8, help="photons per GPU per step")
+    ap.add_argument("--math", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--ref-photons", type=float, default=1e7)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local, dist
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"sm_max_mhz": 1965.0, "fallback": True}
+
+
+def cpu_baseline(w, seconds: float) -> dict:
+    """The oracle (scalar C, OpenMP over streams) on the first streams of the same job."""
+    import oracle
+    from ymc3d_b200 import default_table
+    g, p, job = w.geoms[0], w.props[0], w.jobs[0]
+    table = default_table()
+    cores = os.cpu_count() or 1
+    S = job.num_streams()
+    count = max(cores * 4, 64)
+    while True:
+        t0 = time.perf_counter()
+        r = oracle.run(g.tissue, g.dx, g.dy, g.dz, p.mua, p.mus, p.g, p.n, int(job.photons), S,
+                       int(job.seed), table, beam=0, threads=cores, first=0, count=count)
+        dt = time.perf_counter() - t0
+        if dt > seconds / 4 or count * (job.photons // S) >= 5_000_000:
+            break
+        count = int(count * min(8.0, max(2.0, seconds / 2 / max(dt, 1e-3))))
+    nph = r["totals"]["photons"]
+    return {"value": nph / dt, "unit": "photons/s", "cores": cores, "kind": "port",
+            "sample": f"{nph} photons (first {count} RNG streams of the same job), "
+                      f"{r['totals']['steps']} steps, {dt:.2f} s",
+            "steps_per_s": r["totals"]["steps"] / dt}
+
+
+def run_ours(args):
+    import torch
+
+    import ymc3d_b200 as m
+    from ymc3d_b200.workloads import layered_vessel
+
+    world, rank, local, dist = dist_setup(args)
+    dev = local
+    torch.cuda.set_device(dev)
+    per_gpu = int(args.photons)
+    w = layered_vessel(photons=per_gpu * world)
+    job = w.jobs[0]
+    S = job.num_streams()
+    shard = m.Job(job.geom, job.props, job.photons, job.seed, job.beam, S,
+                  stream_first=rank * S // world,
+                  stream_count=(rank + 1) * S // world - rank * S // world)
+    g = w.geoms[0]
+    pinned = torch.empty(g.tissue.size, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = g.tissue.reshape(-1)
+    geom = m.Geometry(pinned.numpy().reshape(g.tissue.shape), g.dx, g.dy, g.dz)
+    table = m.default_table()
+    pinned_tab = torch.empty(len(table), dtype=torch.int32, pin_memory=True)
+    pinned_tab.numpy().view(np.uint32)[:] = table
+    table_p = pinned_tab.numpy().view(np.uint32)
+
+    plan = m.Plan([geom], w.props, [shard], table=table_p, math=args.math, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    nb = g.tissue.shape[1] * g.tissue.shape[2]
+
+    def exchange(res):
+        """sum the shards' integer tallies over NCCL (the path's exchange step)"""
+        if world == 1:
+            return res
+        r = res[0]
+        t = torch.from_numpy(np.concatenate([r.drs.view(np.int64).reshape(-1),
+                                             r.drs_sq.view(np.int64).reshape(-1),
+                                             r.trans.view(np.int64).reshape(-1),
+                                             np.array([r.totals[k] for k in m.TOTAL_FIELDS],
+                                                      np.uint64).view(np.int64)])).cuda(dev)
+        dist.all_reduce(t)
+        a = t.cpu().numpy().view(np.uint64)
+        r.drs, r.drs_sq, r.trans = (a[:nb].reshape(r.drs.shape), a[nb:2 * nb].reshape(r.drs.shape),
+                                    a[2 * nb:3 * nb].reshape(r.drs.shape))
+        r.totals = {k: int(v) for k, v in zip(m.TOTAL_FIELDS, a[3 * nb:])}
+        return res
+
+    for _ in range(args.warmup):
+        plan.execute(stream.cuda_stream)
+        exchange(plan.read())
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    times, steps_tot, fresnel_tot, photons_tot = [], 0, 0, 0
+    launches = 0
+    with ClockSampler(dev) as clocks:
+        for k in range(args.steps):
+            flush.fill_(k & 0xff)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.execute(stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            launches += 1
+            times.append(e0.elapsed_time(e1) / 1e3)
+            res = exchange(plan.read())
+            steps_tot += res[0].totals["steps"]
+            fresnel_tot += res[0].totals["fresnel"]
+            photons_tot += res[0].totals["photons"]
+    torch.cuda.synchronize(dev)
+    t_step = sum(times) / len(times)
+    if dist:
+        tt = torch.tensor([t_step], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step = float(tt.item())
+    photons_step = photons_tot / args.steps  # whole job after the exchange
+    value = photons_step / t_step
+
+    e2e = None
+    if not args.no_e2e:
+        e2e_times = []
+        h2d = g.tissue.size + table_p.nbytes + sum(p.mua.nbytes * 4 for p in w.props)
+        d2h = 3 * nb * 8 + 14 * 8
+        for k in range(max(1, args.steps)):
+            flush.fill_(k & 0xff)
+            torch.cuda.synchronize(dev)
+            if dist:
+                dist.barrier()
+            t0 = time.perf_counter()
+            res = m.run([geom], w.props, [shard], table=table_p, math=args.math, device=dev)
+            exchange(res)
+            e2e_times.append(time.perf_counter() - t0)
+        te = sum(e2e_times) / len(e2e_times)
+        if dist:
+            tt = torch.tensor([te], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": photons_step / te, "unit": "photons/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": te * 1e3,
+               "timing": "host clock around the synchronous mc3d_run call (plan, upload, "
+                         "kernel, read-back), max over ranks"}
+
+    if rank != 0:
+        plan.close()
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    pk = peaks()
+    clk = clocks.summary()
+    f_max = float(pk.get("sm_max_mhz", 1965.0)) * 1e6
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    steps_per_s = steps_tot / args.steps / world / t_step  # per GPU
+    fres_per_s = fresnel_tot / args.steps / world / t_step
+    sfu_ops = steps_per_s * SFU_STEP + fres_per_s * SFU_FRESNEL
+    fp32_ops = steps_per_s * (OPS_STEP - SFU_STEP) + fres_per_s * (OPS_FRESNEL - SFU_FRESNEL)
+    sfu_peak = sms * SFU_LANES_PER_SM * f_max
+    fp32_peak = sms * FP32_LANES_PER_SM * f_max
+    traffic = None
+    tp = ROOT / "profiles" / "traffic.json"
+    if tp.exists():
+        try:
+            traffic = json.loads(tp.read_text()).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    block, grid, smem = plan.shape()
+    line = {
+        "metric": "photons/s (layered tissue + vessel, 256x256x128, uniform beam, 1 B200)",
+        "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+u64",
+        "data": "synthetic (seeded layered-tissue geometry, reference input formats)",
+        "config": {"workload": w.name, "photons_per_step": int(photons_step),
+                   "photons_per_gpu": per_gpu, "voxels": list(g.shape), "voxel_mm": g.dx,
+                   "beam": "uniform", "math": args.math, "streams": S,
+                   "launch": {"block": block, "grid": grid, "smem": smem},
+                   "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"{world} ranks, disjoint stream shards, NCCL sum of tallies"},
+        "steps_per_s": steps_per_s * world,
+        "roofline": {"bound": "sfu", "achieved": sfu_ops / 1e9, "peak": sfu_peak / 1e9,
+                     "unit": "Gop/s", "frac": sfu_ops / sfu_peak, "traffic": traffic,
+                     "peak_basis": f"{sms} SMs x {SFU_LANES_PER_SM} SFU lanes x sm_max "
+                                   f"{f_max / 1e6:.0f} MHz (MEASURED_PEAKS.json clock)",
+                     "fp32": {"achieved": fp32_ops / 1e9, "peak": fp32_peak / 1e9,
+                              "frac": fp32_ops / fp32_peak},
+                     "ops_per_step": {"all": OPS_STEP, "sfu": SFU_STEP,
+                                      "fresnel_all": OPS_FRESNEL, "fresnel_sfu": SFU_FRESNEL}},
+        "clocks": clk,
+        "gpu_launches": launches * 2,
+        "e2e": e2e,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
+    plan.close()
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    exe = ROOT / "oracle" / "_ref" / "gpu-mc-ref"
+    if not exe.exists():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/gpu-mc-ref not built (oracle/build_ref.py)"}))
+        return
+    from ymc3d_b200.workloads import layered_vessel, write_geometry_file, write_optprops_file
+    w = layered_vessel(photons=int(args.ref_photons))
+    g = w.geoms[0]
+    rows = np.stack([w.props[0].mua, w.props[0].mus, w.props[0].g, w.props[0].n], 1)[1:]
+    tmp = Path(tempfile.mkdtemp())
+    write_geometry_file(tmp / "geom.bin", g.tissue, g.dx, g.dy, g.dz)
+    write_optprops_file(tmp / "props.bid", rows)
+    secs, fins = [], []
+    for k in range(args.warmup + args.steps):
+        out = tmp / f"r{k}"
+        subprocess.run([str(exe), str(tmp / "geom.bin"), str(tmp / "props.bid"),
+                        str(int(args.ref_photons)), str(1796308352 + k), str(out),
+                        str(exe.parent)], check=True, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
+        raw = (tmp / f"r{k}_ref.bin").read_bytes()
+        fin = int(np.frombuffer(raw, "<i8", 1)[0])
+        s = float(np.frombuffer(raw, "<f8", 1, offset=8)[0])
+        if k >= args.warmup:
+            secs.append(s)
+            fins.append(fin)
+    value = sum(fins) / sum(secs)
+    cores = os.cpu_count() or 1
+    line = {
+        "metric": "photons/s (layered tissue + vessel, 256x256x128, uniform beam, 1 B200)",
+        "value": value, "unit": "photons/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sum(secs) / len(secs) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded layered-tissue geometry, reference input formats)",
+        "config": {"workload": w.name, "photons_per_step": int(args.ref_photons),
+                   "voxels": list(g.shape), "voxel_mm": g.dx, "beam": "uniform",
+                   "parallelism": "single GPU (the reference has no multi-GPU path)"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "photons/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{int(args.ref_photons)} photons per step through the "
+                                   "reference's run_3dmc_gpu (its CUDA kernels on cuda:0, its "
+                                   "OpenMP host tally), wall time of the call"},
+        "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,91 @@
+"""The C ABI library loads without a GPU, exports every function include/*.h
+declares, and rejects bad inputs on the host with the documented status codes."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_gpu
+
+
+def declared_functions():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"^[A-Za-z_][\w \*]*?\b(mc3d_\w+)\s*\(", text, flags=re.M))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported(engine):
+    names = declared_functions()
+    assert len(names) >= 20
+    out = subprocess.run(["nm", "-D", "--defined-only", str(engine.LIB_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\sT\s(\w+)$", out, flags=re.M))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    lib = C.CDLL(str(engine.LIB_PATH))
+    for n in names:
+        getattr(lib, n)
+    assert lib.mc3d_abi_version() == 1
+
+
+def _inputs(engine):
+    g = engine.Geometry(np.ones((4, 4, 4), np.uint8), 0.1, 0.1, 0.1)
+    p = engine.OpticalProps.from_tissues([(0.1, 10, 0.9, 1.4)])
+    return g, p
+
+
+def _status(engine, fn):
+    try:
+        fn()
+    except engine.Mc3dError as e:
+        return e.status
+    return 0
+
+
+def test_host_side_validation(engine, table):
+    g, p = _inputs(engine)
+    run = engine.run
+    J = engine.Job
+    assert _status(engine, lambda: run([g], [p], [J(photons=10, seed=0)], table)) == -5
+    assert _status(engine, lambda: run([g], [p], [J(photons=10, seed=(4294967117 << 32))],
+                                       table)) == -5
+    assert _status(engine, lambda: run([g], [p], [J(photons=10)], table[:1])) == -6
+    bad_tab = table[:10].copy()
+    bad_tab[3] = 1
+    assert _status(engine, lambda: run([g], [p], [J(photons=10)], bad_tab)) == -6
+    g2 = engine.Geometry(np.full((4, 4, 4), 3, np.uint8), 0.1, 0.1, 0.1)
+    assert _status(engine, lambda: run([g2], [p], [J(photons=10)], table)) == -3
+    only_air = engine.OpticalProps(np.zeros(1), np.zeros(1), np.zeros(1), np.ones(1))
+    assert _status(engine, lambda: run([g], [only_air], [J(photons=10)], table)) == -4
+    g0 = engine.Geometry(np.ones((4, 4, 4), np.uint8), 0.0, 0.1, 0.1)
+    assert _status(engine, lambda: run([g0], [p], [J(photons=10)], table)) == -2
+    assert _status(engine, lambda: run([g], [p], [J(geom=1, photons=10)], table)) == -1
+    assert _status(engine, lambda: run([g], [p], [J(photons=10, streams=5, stream_first=3,
+                                                    stream_count=4)], table)) == -1
+    assert _status(engine, lambda: run([g], [p], [J(photons=10)], table, block=100)) == -1
+    big = [engine.OpticalProps.from_tissues([(0.1, 10, 0.9, 1.4)] * 255)] * 60
+    assert _status(engine, lambda: run([g], big, [J(photons=10)], table)) == -11
+    if not has_gpu():
+        assert _status(engine, lambda: run([g], [p], [J(photons=10)], table)) == -8
+
+
+def test_reference_shaped_entry_needs_table(engine, tmp_path, monkeypatch):
+    """mc3d_run_3dmc_gpu reads ./safeprimes_base32.txt like rng_init
+    (src/mc3d_rng.cu:16) and reports a missing file instead of exiting"""
+    monkeypatch.chdir(tmp_path)
+    g, p = _inputs(engine)
+    tt = g.tissue.astype(np.int32)
+    geo = engine.CRefGeometry(0.1, 0.1, 0.1, 0.4, 0.4, 0.4, 4, 4, 4, tt.ctypes.data)
+    props = engine.CRefOptProps(2, p.n.ctypes.data, p.mua.ctypes.data, p.mus.ctypes.data,
+                                p.g.ctypes.data, 0)
+    R = np.zeros(16)
+    fin = C.c_int(0)
+    st = engine.lib().mc3d_run_3dmc_gpu(geo, props, 100, R.ctypes.data, None, None, None, None,
+                                        C.byref(fin))
+    assert st == -6

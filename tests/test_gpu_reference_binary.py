@@ -1,0 +1,77 @@
+"""The engine against the reference's own run_3dmc_gpu, compiled from its sources
+(oracle/_ref/gpu-mc-ref) and run on the same GPU: per-bin diffuse reflectance
+agrees within 3 sigma in the chi-square sense (the reference is uniform-beam only;
+its pencil branch is compiled out)."""
+from __future__ import annotations
+
+import subprocess
+
+import numpy as np
+import pytest
+from scipy import stats
+
+import ymc3d_b200 as m
+from conftest import ROOT
+from helpers import superbin
+from ymc3d_b200.workloads import (LAYER_ROWS, layered_vessel_geometry, read_drs_file,
+                                  write_geometry_file, write_optprops_file)
+
+pytestmark = pytest.mark.gpu
+
+REF_BIN = ROOT / "oracle" / "_ref" / "gpu-mc-ref"
+
+
+def run_reference(tmp_path, geom, rows, photons, seed):
+    assert REF_BIN.exists(), "oracle/_ref/gpu-mc-ref missing: run oracle/build_ref.py"
+    gp, pp = tmp_path / "geom.bin", tmp_path / "props.bid"
+    write_geometry_file(gp, geom.tissue, geom.dx, geom.dy, geom.dz)
+    write_optprops_file(pp, rows)
+    out = tmp_path / "ref"
+    subprocess.run([str(REF_BIN), str(gp), str(pp), str(photons), str(seed), str(out),
+                    str(REF_BIN.parent)], check=True, capture_output=True, timeout=900)
+    raw = (tmp_path / "ref_ref.bin").read_bytes()
+    fin = int(np.frombuffer(raw, "<i8", 1)[0])
+    nx, ny = np.frombuffer(raw, "<i4", 2, offset=16)
+    R = np.frombuffer(raw, "<f8", int(nx * ny), offset=24).reshape(int(ny), int(nx))
+    drs, _, _ = read_drs_file(tmp_path / "ref_drs.bin")
+    assert np.allclose(drs, R / fin)
+    return R, fin
+
+
+def compare(engine_res, R_ref, n_ref, f):
+    """chi-square of superbinned R/N; the reference keeps no sum W^2, so its
+    per-bin variance is the engine's scaled to the reference's photon count"""
+    s = superbin(engine_res.drs.astype(np.float64), f) / m.WEIGHT_SCALE
+    q = superbin(engine_res.drs_sq.astype(np.float64), f) / m.WEIGHT_SCALE
+    n = engine_res.photons
+    ra, rb = s / n, superbin(R_ref, f) / n_ref
+    var_per_photon = np.maximum(q / n - ra ** 2, 0)
+    var = var_per_photon / n + var_per_photon / n_ref
+    ok = (ra > 1e-6) & (var > 0)
+    chi2 = float(np.sum((ra[ok] - rb[ok]) ** 2 / var[ok]))
+    dof = int(ok.sum())
+    return chi2, dof, float(stats.chi2.sf(chi2, dof))
+
+
+def test_layered_vessel_vs_reference(tmp_path, table):
+    g = layered_vessel_geometry(64, 64, 32, 0.08)
+    R, fin = run_reference(tmp_path, g, LAYER_ROWS, 1_000_000, 1796308352)
+    assert fin >= 1_000_000
+    r = m.run([g], [m.OpticalProps.from_tissues(LAYER_ROWS)],
+              [m.Job(0, 0, 4_000_000, 12345, "uniform")], table=table)[0]
+    chi2, dof, pv = compare(r, R, fin, 8)
+    assert dof >= 32 and pv > 1e-4, (chi2, dof, pv)
+    total_ref = R.sum() / fin
+    total = r.drs.sum() / m.WEIGHT_SCALE / r.photons
+    sigma = np.sqrt(total * (1 - total) * (1 / fin + 1 / r.photons))
+    assert abs(total - total_ref) < 4 * sigma, (total, total_ref, sigma)
+
+
+def test_homogeneous_vs_reference(tmp_path, table):
+    g = m.Geometry(np.ones((32, 32, 32), np.uint8), 0.1, 0.1, 0.1)
+    rows = [(0.05, 10.0, 0.9, 1.4)]
+    R, fin = run_reference(tmp_path, g, rows, 500_000, 20240601)
+    r = m.run([g], [m.OpticalProps.from_tissues(rows)],
+              [m.Job(0, 0, 2_000_000, 777, "uniform")], table=table)[0]
+    chi2, dof, pv = compare(r, R, fin, 4)
+    assert dof >= 32 and pv > 1e-4, (chi2, dof, pv)

@@ -1,0 +1,83 @@
+"""Fast-math kernel: statistical parity, exact conservation and bit-reproducible
+tallies across launch shapes and batching."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import ymc3d_b200 as m
+from helpers import drs_chi2, oracle_job, residual, total_z
+
+pytestmark = pytest.mark.gpu
+
+
+def layered_small():
+    from ymc3d_b200.workloads import LAYER_ROWS, layered_vessel_geometry
+    return layered_vessel_geometry(64, 64, 32, 0.08), m.OpticalProps.from_tissues(LAYER_ROWS)
+
+
+def test_fast_vs_exact_chi2(table):
+    g, p = layered_small()
+    fast = m.run([g], [p], [m.Job(0, 0, 2_000_000, 5, "uniform")], table=table, math="fast")[0]
+    exact = m.run([g], [p], [m.Job(0, 0, 2_000_000, 6, "uniform")], table=table,
+                  math="exact")[0]
+    chi2, dof, pv = drs_chi2(fast.drs, fast.drs_sq, fast.photons, exact.drs, exact.drs_sq,
+                             exact.photons, f=8)
+    assert dof > 20 and pv > 1e-4, (chi2, dof, pv)
+    for key in ("r_in", "absorbed"):
+        assert abs(total_z(fast.totals, exact.totals, key)) < 5
+
+
+def test_fast_vs_oracle_chi2(table):
+    g, p = m.Geometry(np.ones((32, 32, 32), np.uint8), 0.1, 0.1, 0.1), \
+        m.OpticalProps.from_tissues([(0.05, 10.0, 0.9, 1.4)])
+    job = m.Job(0, 0, 40_000, 2024, "pencil")
+    fast = m.run([g], [p], [job], table=table, math="fast")[0]
+    o = oracle_job(g, p, m.Job(0, 0, 40_000, 2025, "pencil"), table)
+    chi2, dof, pv = drs_chi2(fast.drs, fast.drs_sq, fast.photons, o["drs"], o["drs_sq"],
+                             o["totals"]["photons"], f=4)
+    assert dof > 10 and pv > 1e-4, (chi2, dof, pv)
+    assert abs(total_z(fast.totals, o["totals"], "r_in")) < 5
+
+
+def test_conservation_exact(table):
+    g, p = layered_small()
+    r = m.run([g], [p], [m.Job(0, 0, 1_000_000, 77, "uniform")], table=table)[0]
+    t = r.totals
+    assert t["photons"] == 1_000_000
+    assert residual(t) == 0
+    assert int(r.drs.sum()) == t["r_in"]
+    assert int(r.trans.sum()) == t["t_in"]
+    assert t["w_launched"] > 0 and t["steps"] > t["photons"]
+
+
+@pytest.mark.parametrize("block,bps", [(64, 1), (128, 3), (256, 0), (96, 2)])
+def test_launch_shape_reproducible(table, block, bps):
+    g, p = layered_small()
+    job = m.Job(0, 0, 300_000, 4242, "uniform")
+    base = m.run([g], [p], [job], table=table)[0]
+    r = m.run([g], [p], [job], table=table, block=block, blocks_per_sm=bps)[0]
+    assert r.totals == base.totals
+    assert np.array_equal(r.drs, base.drs) and np.array_equal(r.drs_sq, base.drs_sq)
+
+
+def test_batched_equals_separate(table):
+    from ymc3d_b200.workloads import sweep
+    w = sweep(njobs=6, photons_lo=2e4, photons_hi=2e5)
+    together = m.run(w.geoms, w.props, w.jobs, table=table)
+    for job, r in zip(w.jobs, together):
+        alone = m.run(w.geoms, [w.props[job.props]], [m.Job(0, 0, job.photons, job.seed,
+                                                             job.beam)], table=table)[0]
+        assert r.totals == alone.totals
+        assert np.array_equal(r.drs, alone.drs)
+
+
+def test_plan_reexecute_identical(table):
+    g, p = layered_small()
+    plan = m.Plan([g], [p], [m.Job(0, 0, 200_000, 9, "uniform")], table=table)
+    plan.execute()
+    a = plan.read()[0]
+    plan.execute()
+    b = plan.read()[0]
+    plan.close()
+    assert a.totals == b.totals and np.array_equal(a.drs, b.drs)

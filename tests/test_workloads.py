@@ -1,0 +1,44 @@
+"""The seeded workload generators and the reference-format writers."""
+from __future__ import annotations
+
+import numpy as np
+
+from ymc3d_b200 import workloads as W
+
+
+def test_layered_vessel_geometry():
+    g = W.layered_vessel_geometry()
+    nx, ny, nz = g.shape
+    assert (nx, ny, nz) == (256, 256, 128) and g.dx == 0.02
+    col = g.tissue[:, 0, 0]
+    assert np.all(col[:5] == 1) and np.all(col[5:105] == 2) and np.all(col[105:] == 3)
+    zc, yc = (np.arange(nz) + 0.5) * 0.02, (np.arange(ny) + 0.5) * 0.02
+    in_vessel = ((yc[None, :] - 2.56) ** 2 + (zc[:, None] - 0.5) ** 2) <= 0.09
+    assert np.array_equal(g.tissue[:, :, 7] == 4, in_vessel)
+    assert np.all(g.tissue[:, :, 0] == g.tissue[:, :, -1])  # a cylinder along x
+
+
+def test_sweep_and_uneven_ranges():
+    s = W.sweep()
+    assert len(s.jobs) == 128 and len(s.props) == 128
+    ph = np.array([j.photons for j in s.jobs])
+    assert ph.min() >= 1e6 and ph.max() <= 1e8
+    for p in s.props:
+        g = p.g[1]
+        assert 0.7 <= g <= 0.95 and 1e-3 <= p.mua[1] <= 1 and p.n[1] == np.float32(1.4)
+        assert 0.5 <= p.mus[1] * (1 - g) <= 5.0001
+    u = W.uneven(ngeoms=6, max_dim=96)
+    for g, p in zip(u.geoms, u.props):
+        assert g.tissue.max() < p.num_tissue_types <= 9
+
+
+def test_writers_round_trip(engine, tmp_path):
+    g = W.layered_vessel_geometry(40, 30, 20, 0.05)
+    g.tissue[3, 4, 5] = 0
+    W.write_geometry_file(tmp_path / "g.bin", g.tissue, g.dx, g.dy, g.dz)
+    back = engine.geometry_read_from_file(tmp_path / "g.bin")
+    assert np.array_equal(back.tissue, g.tissue) and back.dx == g.dx
+    W.write_optprops_file(tmp_path / "p.bid", W.LAYER_ROWS)
+    p = engine.opticalprops_read_from_file(tmp_path / "p.bid")
+    assert np.allclose(p.mua[1:], [r[0] for r in W.LAYER_ROWS])
+    assert p.n[0] == 1.0 and p.mua[0] == 0

@@ -1,0 +1,536 @@
+/*
+ * mc3d_engine.cuh -- the photon-tracking hot path on sm_100a.
+ *
+ * One persistent kernel runs every photon of every job in a launch.  The unit of
+ * work is an RNG *stream*: stream i of a job owns multiplier a_(i mod M) of the
+ * safe-prime table and runs the job's photons i, i+S, i+2S, ... one after
+ * another, continuing the same multiply-with-carry sequence, exactly as one
+ * photon slot of the reference does (src/mc3d_gpu.cu:74-111, 128-376) minus the
+ * masked steps a frozen slot burns until the next host round trip.  Threads take
+ * streams from a global counter, so the trajectories depend on (table, seed,
+ * photons, streams) only -- never on the grid shape or on scheduling -- and the
+ * tallies, being 64-bit integer sums, are bit-reproducible.
+ *
+ * Per-step physics follows src/mc3d_gpu.cu:175-340 operation for operation,
+ * including its quirks (Fresnel denominator, 0/0 -> transmit at normal incidence,
+ * mirror short-circuit after a Fresnel reflection, freeze one step after entering
+ * air, i/j/k re-derived from the position every 45 steps, the NaN/db==0 quickfix
+ * at the end of each 45-step chunk).  The math policy decides how the elementary
+ * operations are evaluated: MathExact uses correctly rounded IEEE operations and
+ * the reproducible series of mc3d_exactmath.h (bit-identical to the CPU
+ * transcription), MathFast uses the GPU's approximate instructions like the
+ * reference's -use_fast_math build.
+ */
+#ifndef MC3D_ENGINE_CUH
+#define MC3D_ENGINE_CUH
+
+#include <stdint.h>
+#include <cuda_runtime.h>
+#include "mc3d_rng.h"
+#include "mc3d_exactmath.h"
+#include "mc3d_device_types.h"
+
+namespace mc3d {
+
+/* ---------------------------------------------------------------- math policies */
+struct MathExact {
+    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float rsqrt(float x) { return 1.0f / sqrtf(x); }
+    static __device__ __forceinline__ float log(float x) { return mc3d_xm_logf(x); }
+    static __device__ __forceinline__ float acos(float x) { return mc3d_xm_acosf(x); }
+    static __device__ __forceinline__ float sin(float x) { return mc3d_xm_sinf(x); }
+    static __device__ __forceinline__ void sincospi(float x, float *s, float *c)
+    {
+        mc3d_xm_sincospif(x, s, c);
+    }
+};
+
+/* Compiled only in a translation unit built with -use_fast_math, where the
+ * operators and functions below map to the approximate hardware paths. */
+struct MathFast {
+    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
+    static __device__ __forceinline__ float log(float x) { return logf(x); }
+    static __device__ __forceinline__ float acos(float x) { return acosf(x); }
+    static __device__ __forceinline__ float sin(float x) { return sinf(x); }
+    static __device__ __forceinline__ void sincospi(float x, float *s, float *c)
+    {
+        sincospif(x, s, c);
+    }
+};
+
+/* ------------------------------------------------------------ reference constants
+ * src/mc3d_types.h:11-18.  SURVIVAL_CHANCE, W_THRESHOLD and UZ_THRESH are double
+ * literals there, so a float compared with them is widened to double.  No float
+ * lies between each literal and the float bound below, so these float comparisons
+ * decide exactly as the double ones do (the unit tests enumerate the neighbours):
+ *   (double)e <  0.1      <=>  e <  0x1.99999ap-4f   ((float)0.1 is above 0.1)
+ *   (double)w <  0.0001   <=>  w <= 0x1.a36e2ep-14f  ((float)0.0001 is below it)
+ *   (double)u <= 0.99999  <=>  u <= 0x1.fffeb0p-1f   ((float)0.99999 is below it)
+ * The roulette division W / 0.1 stays in double, as in the reference. */
+#define MC3D_SURVIVAL_CHANCE 0.1
+#define MC3D_SURVIVAL_LT_F 0x1.99999ap-4f
+#define MC3D_W_THRESHOLD_LE_F 0x1.a36e2ep-14f
+#define MC3D_UZ_THRESH 0.99999
+#define MC3D_UZ_THRESH_LE_F 0x1.fffeb0p-1f
+#define MC3D_NUM_PHOTON_STEPS 45
+#define MC3D_TISSUE_AIR 0
+
+/* fixed-point weight, 2^-32 resolution */
+static __device__ __forceinline__ uint64_t qw(float w)
+{
+    return __float2ull_rn(w * 4294967296.0f);
+}
+
+/* src/mc3d_gpu.cu:53-63 */
+template <class M>
+static __device__ __forceinline__ int grid_coord(float x, float ux, float d)
+{
+    int i = (int)floorf(M::div(x, d));
+    i += (x == (float)(int)((unsigned)i + 1u) * d);
+    float bmin = (float)i * d;
+    i = ((x > bmin) || ((x == bmin) && (ux >= 0))) ? i : i - 1;
+    return i;
+}
+
+/* src/mc3d_gpu.cu:24-27 with the clamp addressing of the texture (:416-418) */
+static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, int k, float z,
+                                                float uz)
+{
+    int ci = min(max(i, 0), g.nx - 1);
+    int cj = min(max(j, 0), g.ny - 1);
+    int ck = min(max(k, 0), g.nz - 1);
+    int t = __ldg(g.tissue + ((int64_t)ck * g.ny + cj) * g.nx + ci);
+    return ((z <= 0) && (uz < 0)) ? MC3D_TISSUE_AIR : t;
+}
+
+/* src/mc3d_gpu.cu:29-49 */
+template <class M>
+static __device__ __forceinline__ float intersection(const GeomDev &g, int i, int j, int k,
+                                                     float *x, float ux, float *y, float uy,
+                                                     float *z, float uz)
+{
+    float border_x = (float)((ux >= 0) ? (int)((unsigned)i + 1u) : i) * g.dx;
+    float t_x = M::div(border_x - *x, ux);
+    float border_y = (float)((uy >= 0) ? (int)((unsigned)j + 1u) : j) * g.dy;
+    float t_y = M::div(border_y - *y, uy);
+    float border_z = (float)((uz >= 0) ? (int)((unsigned)k + 1u) : k) * g.dz;
+    float t_z = M::div(border_z - *z, uz);
+    float t = fminf(t_x, fminf(t_y, t_z));
+    *x = (t == t_x) ? border_x : *x + ux * t;
+    *y = (t == t_y) ? border_y : *y + uy * t;
+    *z = (t == t_z) ? border_z : *z + uz * t;
+    return t;
+}
+
+/* src/mc3d_gpu.cu:113-126 */
+static __device__ __forceinline__ bool mirror(float *x, float *ux, float length)
+{
+    bool refl = (*x >= length) || (*x <= 0);
+    *x = (*x >= length) ? 2 * length - *x : *x;
+    *x = (*x <= 0) ? fabsf(*x) : *x;
+    *ux = refl ? -1 * (*ux) : *ux;
+    return refl;
+}
+
+struct Photon {
+    float x, y, z, ux, uy, uz, W, s;
+    int i, j, k, tissue;
+};
+
+/* Per-photon weight bookkeeping (fixed point) for the conservation identity
+ *   Q(W0) = absorbed + exit + rr_killed - rr_created + lost. */
+struct PhotonBook {
+    uint64_t killed, created;
+};
+
+/* One step of src/mc3d_gpu.cu:175-340 for a live photon.  Returns true when the
+ * photon froze during this step; *db receives the step's boundary distance. */
+template <class M>
+static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float4 *tab,
+                                                   Photon &p, uint64_t &rx, uint32_t ra,
+                                                   PhotonBook &bk, float *db_out,
+                                                   uint32_t *fresnel_count)
+{
+    const float4 cur = tab[p.tissue]; /* mua, mus, g, n */
+    float ni = cur.w;
+    float nt = ni;
+    float mu_a = cur.x, mu_s = cur.y, gg = cur.z;
+    float mu_t = mu_a + mu_s;
+
+    float newx = p.x, newy = p.y, newz = p.z;
+    float db = intersection<M>(g, p.i, p.j, p.k, &newx, p.ux, &newy, p.uy, &newz, p.uz);
+
+    bool hit = db * mu_t <= p.s;
+    float ds = hit ? db * mu_t : p.s;
+    newx = hit ? newx : p.x + M::div(p.ux * ds, mu_t);
+    newy = hit ? newy : p.y + M::div(p.uy * ds, mu_t);
+    newz = hit ? newz : p.z + M::div(p.uz * ds, mu_t);
+    float s = p.s - ds;
+
+    int nexti = grid_coord<M>(newx, p.ux, g.dx);
+    int nextj = grid_coord<M>(newy, p.uy, g.dy);
+    int nextk = grid_coord<M>(newz, p.uz, g.dz);
+    int next_tissue = tissue_at(g, nexti, nextj, nextk, newz, p.uz);
+    nt = tab[next_tissue].w;
+
+    float tr_ux = p.ux, tr_uy = p.uy, tr_uz = p.uz;
+    bool refl = false;
+    if (ni != nt) { /* src/mc3d_gpu.cu:226-257 */
+        float cos_ai = (p.i != nexti) ? p.ux : ((p.j != nextj) ? p.uy : p.uz);
+        cos_ai = fabsf(cos_ai);
+        cos_ai = (cos_ai > 1) ? 1 : cos_ai;
+        float ai = M::acos(cos_ai);
+        float ni_nt = M::div(ni, nt);
+        float sin_ai = M::sin(ai);
+        float sin_at = ni_nt * sin_ai;
+        float cos_at = M::sqrt(1.0f - sin_at * sin_at);
+        float R1 = M::div(sin_ai * cos_at - cos_ai * sin_at, sin_ai * cos_at + cos_ai * sin_at);
+        float R2 = M::div(cos_ai * cos_at - sin_ai * sin_at, cos_ai * cos_at + sin_at * sin_at);
+        float R = 0.5 * R1 * R1 * (1.0f + R2 * R2);
+        R = (sin_at > 1) ? 1 : R;
+        R = (ni == nt) ? 0 : R;
+        float eps = mc3d_rand_co(&rx, ra);
+        refl = eps < R;
+        tr_ux = refl ? p.ux * ((p.i == nexti) ? 1 : -1)
+                     : ((p.i != nexti) ? copysignf(cos_at, p.ux * cos_at) : p.ux * ni_nt);
+        tr_uy = refl ? p.uy * ((p.j == nextj) ? 1 : -1)
+                     : (((p.j != nextj) && (p.i == nexti)) ? copysignf(cos_at, p.uy * cos_at)
+                                                           : p.uy * ni_nt);
+        tr_uz = refl ? p.uz * ((p.k == nextk) ? 1 : -1)
+                     : (((p.k != nextk) && (p.j == nextj) && (p.i == nexti))
+                            ? copysignf(cos_at, p.uz * cos_at)
+                            : p.uz * ni_nt);
+        (*fresnel_count)++;
+    }
+
+    /* absorption, src/mc3d_gpu.cu:262-263 */
+    float W = p.W;
+    float dW = (mu_t > 0) ? M::div(mu_a, mu_t) * W : 0;
+    W = W - dW * (float)(!hit);
+
+    /* russian roulette, src/mc3d_gpu.cu:275-277 */
+    float eps = mc3d_rand_co(&rx, ra);
+    bool roulette = (W <= MC3D_W_THRESHOLD_LE_F) && (!hit) && (mu_t != 0);
+    if (roulette) {
+        float newW = (eps < MC3D_SURVIVAL_LT_F) ? (float)((double)W / MC3D_SURVIVAL_CHANCE) : 0.0f;
+        if (newW == 0.0f) bk.killed += qw(W);
+        else bk.created += qw(newW) - qw(W);
+        W = newW;
+    }
+
+    /* Henyey-Greenstein, src/mc3d_gpu.cu:282-294 */
+    float costheta = M::div(1 - gg * gg, 1 - gg + 2 * gg * mc3d_rand_oc(&rx, ra));
+    costheta = M::div(1.0f, 2 * gg) * (1 + gg * gg - costheta * costheta);
+    float sintheta = M::sqrt(1 - costheta * costheta);
+    float phi_divpi = 2 * mc3d_rand_co(&rx, ra);
+    float cosphi, sinphi;
+    M::sincospi(phi_divpi, &sinphi, &cosphi);
+    float invsqrt = M::rsqrt(1 - p.uz * p.uz);
+    bool steep = !(fabsf(p.uz) <= MC3D_UZ_THRESH_LE_F);
+    float sc_ux = !steep ? sintheta * (p.ux * p.uz * cosphi - p.uy * sinphi) * invsqrt +
+                               p.ux * costheta
+                         : sintheta * cosphi;
+    float sc_uy = !steep ? sintheta * (p.uy * p.uz * cosphi + p.ux * sinphi) * invsqrt +
+                               p.uy * costheta
+                         : sintheta * sinphi;
+    float sc_uz = !steep ? -1 * M::sqrt(1 - p.uz * p.uz) * sintheta * cosphi + p.uz * costheta
+                         : copysignf(costheta, costheta * p.uz);
+
+    float nux = (!hit) ? sc_ux : tr_ux;
+    float nuy = (!hit) ? sc_uy : tr_uy;
+    float nuz = (!hit) ? sc_uz : tr_uz;
+    const float zero_thresh = (float)(1 - MC3D_UZ_THRESH);
+    nux = (fabsf(nux) < zero_thresh) ? 0 : nux;
+    nuy = (fabsf(nuy) < zero_thresh) ? 0 : nuy;
+    nuz = (fabsf(nuz) < zero_thresh) ? 0 : nuz;
+    float norm = M::rsqrt(nux * nux + nuy * nuy + nuz * nuz);
+    nux *= norm;
+    nuy *= norm;
+    nuz *= norm;
+
+    bool freeze = (W <= 0) || (mu_t == 0);
+    p.ux = !freeze ? nux : p.ux;
+    p.uy = !freeze ? nuy : p.uy;
+    p.uz = !freeze ? nuz : p.uz;
+
+    float e2 = mc3d_rand_oc(&rx, ra);
+    float newS = (W > 0) ? -M::log(e2) : 0;
+    p.s = (freeze || hit) ? s : newS;
+    p.W = W;
+
+    p.x = !freeze ? newx : p.x;
+    p.y = !freeze ? newy : p.y;
+    p.z = !freeze ? newz : p.z;
+
+    /* mirror boundary conditions, short-circuited as in src/mc3d_gpu.cu:330 */
+    refl = refl || mirror(&p.x, &p.ux, g.Lx) || mirror(&p.y, &p.uy, g.Ly);
+
+    bool keep = (hit && refl) || freeze;
+    p.i = keep ? p.i : nexti;
+    p.j = keep ? p.j : nextj;
+    p.k = keep ? p.k : nextk;
+    p.tissue = keep ? p.tissue : next_tissue;
+    *db_out = db;
+    return freeze;
+}
+
+/* i, j, k and tissue from the position, as at the start of every launch of
+ * photontrack_step (src/mc3d_gpu.cu:168-171). */
+template <class M>
+static __device__ __forceinline__ void derive_cell(const GeomDev &g, Photon &p)
+{
+    p.i = grid_coord<M>(p.x, p.ux, g.dx);
+    p.j = grid_coord<M>(p.y, p.uy, g.dy);
+    p.k = grid_coord<M>(p.z, p.uz, g.dz);
+    p.tissue = tissue_at(g, p.i, p.j, p.k, p.z, p.uz);
+}
+
+static __device__ __forceinline__ bool finite_state(const Photon &p)
+{
+    return isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(p.s) &&
+           isfinite(p.ux) && isfinite(p.uy) && isfinite(p.uz);
+}
+
+/* The NaN/Inf/db==0 quickfix run after each 45-step launch (src/mc3d_gpu.cu:343-353).
+ * Returns true (and zeroes the photon) when it fires. */
+static __device__ __forceinline__ bool quickfix(Photon &p, float db)
+{
+    if (!finite_state(p) || db == 0) {
+        p.x = 0; p.y = 0; p.z = 0;
+        p.ux = 0; p.uy = 0; p.uz = 1;
+        p.W = 0; p.s = 0;
+        return true;
+    }
+    return false;
+}
+
+/* The steps a frozen slot keeps executing until the end of its 45-step launch.
+ * They change nothing but the mirror (which flips u while the photon sits on a
+ * lateral face) and the boundary distance the quickfix looks at. */
+template <class M>
+static __device__ __forceinline__ float masked_steps(const GeomDev &g, Photon &p, int masked,
+                                                     float db)
+{
+    for (int t = 0; t < masked; t++) {
+        float nx_ = p.x, ny_ = p.y, nz_ = p.z;
+        db = intersection<M>(g, p.i, p.j, p.k, &nx_, p.ux, &ny_, p.uy, &nz_, p.uz);
+        if (!mirror(&p.x, &p.ux, g.Lx)) mirror(&p.y, &p.uy, g.Ly);
+    }
+    return db;
+}
+
+/* --------------------------------------------------------------- kernel body */
+struct ThreadAcc {
+    uint64_t photons, steps, w_launched, r_in, r_out, t_in, t_out, absorbed;
+    uint64_t rr_killed, rr_created, lost, capped, quickfix, fresnel;
+};
+
+static __device__ __forceinline__ void acc_clear(ThreadAcc &a)
+{
+    a.photons = a.steps = a.w_launched = a.r_in = a.r_out = a.t_in = a.t_out = a.absorbed = 0;
+    a.rr_killed = a.rr_created = a.lost = a.capped = a.quickfix = a.fresnel = 0;
+}
+
+static __device__ __forceinline__ void acc_flush(ThreadAcc &a, unsigned long long *tot)
+{
+    if (a.photons == 0 && a.steps == 0) return;
+    atomicAdd(tot + 0, (unsigned long long)a.photons);
+    atomicAdd(tot + 1, (unsigned long long)a.steps);
+    atomicAdd(tot + 2, (unsigned long long)a.w_launched);
+    atomicAdd(tot + 3, (unsigned long long)a.r_in);
+    if (a.r_out) atomicAdd(tot + 4, (unsigned long long)a.r_out);
+    if (a.t_in) atomicAdd(tot + 5, (unsigned long long)a.t_in);
+    if (a.t_out) atomicAdd(tot + 6, (unsigned long long)a.t_out);
+    atomicAdd(tot + 7, (unsigned long long)a.absorbed);
+    if (a.rr_killed) atomicAdd(tot + 8, (unsigned long long)a.rr_killed);
+    if (a.rr_created) atomicAdd(tot + 9, (unsigned long long)a.rr_created);
+    if (a.lost) atomicAdd(tot + 10, (unsigned long long)a.lost);
+    if (a.capped) atomicAdd(tot + 11, (unsigned long long)a.capped);
+    if (a.quickfix) atomicAdd(tot + 12, (unsigned long long)a.quickfix);
+    if (a.fresnel) atomicAdd(tot + 13, (unsigned long long)a.fresnel);
+    acc_clear(a);
+}
+
+/* job owning global stream index gs (binary search over the stream prefix) */
+static __device__ __forceinline__ int find_job(const JobDev *jobs, int njobs, int64_t gs)
+{
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].stream_base <= gs) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+/* initial packed state of stream `local` of job `jb` (gpumcml_rng/gpumcml_rng.cu:95-114),
+ * honouring the seeding attempts that earlier streams of the job rejected */
+static __device__ __forceinline__ uint64_t stream_seed(const KernelParams &P, const JobDev &jb,
+                                                       int64_t local, uint32_t fora)
+{
+    int64_t offset = 0;
+    int lo = 0, hi = jb.rej_count - 1;
+    while (lo <= hi) { /* last listed stream <= local */
+        int mid = (lo + hi) >> 1;
+        if (P.rejections[jb.rej_offset + mid].stream <= local) {
+            offset = P.rejections[jb.rej_offset + mid].cum;
+            lo = mid + 1;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    uint64_t xs = mc3d_seed_jump(&P.seed, jb.seed, (uint64_t)(local + offset));
+    return mc3d_seed_attempt(xs, P.seed.begin, fora);
+}
+
+template <class M>
+__device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
+{
+    extern __shared__ float4 sh_tab[];
+    for (int t = threadIdx.x; t < P.props_entries; t += blockDim.x) sh_tab[t] = P.props_table[t];
+    __syncthreads();
+
+    ThreadAcc acc;
+    acc_clear(acc);
+    int job = -1;
+    unsigned long long *job_tot = nullptr;
+    GeomDev g;
+    const float4 *tab = sh_tab;
+    JobDev jb;
+    int64_t left = 0, local = 0, kphot = 0;
+    uint64_t rx = 0;
+    uint32_t ra = 1;
+    Photon p;
+    PhotonBook bk;
+    bool alive = false;
+    int chunk = 0;
+    uint32_t psteps = 0;
+    uint32_t fresnel = 0;
+    uint64_t qw0 = 0;
+    const int64_t max_steps = P.max_steps;
+
+    for (;;) {
+        if (!alive) {
+            if (left == 0) {
+                acc.fresnel += fresnel;
+                fresnel = 0;
+                if (job_tot) acc_flush(acc, job_tot);
+                if (P.cancel && *((volatile const int *)P.cancel)) break;
+                int64_t gs = (int64_t)atomicAdd((unsigned long long *)P.work_counter, 1ull);
+                if (gs >= P.total_streams) break;
+                job = find_job(P.jobs, P.njobs, gs);
+                jb = P.jobs[job];
+                g = P.geoms[jb.geom];
+                tab = sh_tab + jb.props_offset;
+                job_tot = P.totals + (int64_t)job * MC3D_NUM_TOTALS;
+                local = gs - jb.stream_base + jb.stream_first;
+                left = jb.per_stream + (local < jb.remainder ? 1 : 0);
+                kphot = 0;
+                ra = P.multipliers[1 + (local % (P.num_multipliers - 1))];
+                rx = stream_seed(P, jb, local, ra);
+                if (left == 0) continue;
+            }
+            /* photontrack_reinitialize, src/mc3d_gpu.cu:74-111 */
+            if (jb.beam == 0) {
+                p.x = g.Lx * mc3d_rand_co(&rx, ra);
+                p.y = g.Ly * mc3d_rand_co(&rx, ra);
+            } else {
+                p.x = g.Lx / 2;
+                p.y = g.Ly / 2;
+            }
+            p.z = 0;
+            p.ux = 0; p.uy = 0; p.uz = 1;
+            /* specular reflection from air into tissue type 1 (src/mc3d_gpu.cu:67-70, 500) */
+            float rsp = M::div(tab[MC3D_TISSUE_AIR].w - tab[1].w, tab[MC3D_TISSUE_AIR].w + tab[1].w);
+            rsp = rsp * rsp;
+            p.W = 1.0f - rsp;
+            qw0 = qw(p.W);
+            p.s = -M::log(mc3d_rand_oc(&rx, ra));
+            derive_cell<M>(g, p);
+            bk.killed = 0; bk.created = 0;
+            chunk = 0;
+            psteps = 0;
+            alive = true;
+            left--;
+            acc.w_launched += qw0;
+        }
+
+        float db;
+        bool froze = photon_step<M>(g, tab, p, rx, ra, bk, &db, &fresnel);
+        chunk++;
+        psteps++;
+
+        bool done = false;
+        uint64_t lost = 0;
+        if (froze) {
+            db = masked_steps<M>(g, p, MC3D_NUM_PHOTON_STEPS - chunk, db);
+            float w_before = p.W;
+            if (quickfix(p, db)) { acc.quickfix++; lost = qw(w_before); }
+            done = true;
+        } else if (chunk == MC3D_NUM_PHOTON_STEPS) {
+            float w_before = p.W;
+            if (quickfix(p, db)) { acc.quickfix++; lost = qw(w_before); done = true; }
+            else { derive_cell<M>(g, p); chunk = 0; }
+        }
+        if (!done && (int64_t)psteps >= max_steps) {
+            lost = qw(p.W);
+            p.W = 0;
+            acc.capped++;
+            done = true;
+        }
+        if (done) {
+            /* photon_detector, src/mc3d_photons.cu:151-171 */
+            int ix = grid_coord<M>(p.x, p.ux, g.dx);
+            int iy = grid_coord<M>(p.y, p.uy, g.dy);
+            bool inside = (ix >= 0) && (iy >= 0) && (ix < g.nx) && (iy < g.ny);
+            uint64_t q = qw(p.W);
+            int64_t bin = jb.bin_offset + (int64_t)iy * g.nx + ix;
+            if (p.z <= 0) {
+                if (inside) {
+                    if (q) {
+                        atomicAdd(P.drs + bin, (unsigned long long)q);
+                        atomicAdd(P.drs_sq + bin, (unsigned long long)qw(p.W * p.W));
+                    }
+                    acc.r_in += q;
+                } else {
+                    acc.r_out += q;
+                }
+            } else {
+                if (inside) {
+                    if (q) atomicAdd(P.trans + bin, (unsigned long long)q);
+                    acc.t_in += q;
+                } else {
+                    acc.t_out += q;
+                }
+            }
+            acc.absorbed += qw0 - q - bk.killed + bk.created - lost;
+            acc.rr_killed += bk.killed;
+            acc.rr_created += bk.created;
+            acc.lost += lost;
+            acc.photons++;
+            acc.steps += psteps;
+            if (P.photon_log) {
+                int64_t pid = jb.photon_base + local + kphot * jb.streams;
+                PhotonRecord r;
+                r.x = p.x; r.y = p.y; r.z = p.z;
+                r.ux = p.ux; r.uy = p.uy; r.uz = p.uz;
+                r.W = p.W; r.s = p.s;
+                r.steps = psteps;
+                r.tissue = (uint32_t)p.tissue;
+                r.rng = rx;
+                P.photon_log[pid] = r;
+            }
+            kphot++;
+            alive = false;
+        }
+    }
+    acc.fresnel += fresnel;
+    if (job_tot) acc_flush(acc, job_tot);
+}
+
+} /* namespace mc3d */
+
+#endif /* MC3D_ENGINE_CUH */

@@ -1,0 +1,40 @@
+/*
+ * mc3d_kernel_fast.cu -- the photon kernel with the GPU's approximate math.
+ * Built with -use_fast_math like the reference (CMakeLists.txt:18): divisions,
+ * sqrtf, logf and sinf map to the approximate hardware paths.
+ */
+#include "mc3d_engine.cuh"
+#include "mc3d_launch.h"
+
+namespace mc3d {
+
+__global__ void __launch_bounds__(256) photon_kernel_fast(const __grid_constant__ KernelParams P)
+{
+    photon_kernel_body<MathFast>(P);
+}
+
+cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_t smem,
+                               cudaStream_t stream)
+{
+    photon_kernel_fast<<<grid, block, smem, stream>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t occupancy_photon_fast(int block, size_t smem, int *blocks_per_sm)
+{
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, photon_kernel_fast, block,
+                                                         smem);
+}
+
+cudaError_t smem_limit_photon_fast(size_t smem)
+{
+    return cudaFuncSetAttribute(photon_kernel_fast, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem);
+}
+
+cudaError_t attributes_photon_fast(cudaFuncAttributes *attr)
+{
+    return cudaFuncGetAttributes(attr, photon_kernel_fast);
+}
+
+} /* namespace mc3d */

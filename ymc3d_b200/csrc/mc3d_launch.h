@@ -1,0 +1,37 @@
+/*
+ * mc3d_launch.h -- launchers of the device code, one per translation unit.
+ * The fast and exact photon kernels live in separate files because their math
+ * depends on compile flags (-use_fast_math vs -fmad=false).
+ */
+#ifndef MC3D_LAUNCH_H
+#define MC3D_LAUNCH_H
+
+#include <cuda_runtime.h>
+#include "mc3d_device_types.h"
+
+namespace mc3d {
+
+cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_t smem,
+                               cudaStream_t stream);
+cudaError_t launch_photon_exact(const KernelParams &P, int grid, int block, size_t smem,
+                                cudaStream_t stream);
+cudaError_t occupancy_photon_fast(int block, size_t smem, int *blocks_per_sm);
+cudaError_t occupancy_photon_exact(int block, size_t smem, int *blocks_per_sm);
+cudaError_t smem_limit_photon_fast(size_t smem);
+cudaError_t smem_limit_photon_exact(size_t smem);
+cudaError_t attributes_photon_fast(cudaFuncAttributes *attr);
+cudaError_t attributes_photon_exact(cudaFuncAttributes *attr);
+
+/* first rejected seeding attempt per job, assuming none before it (UINT64_MAX if none) */
+cudaError_t launch_seed_scan(const JobDev *jobs, int njobs, const uint32_t *mult,
+                             int64_t nmult, const mc3d_seed_consts &sc, int64_t total_streams,
+                             unsigned long long *first_reject, cudaStream_t stream);
+/* states of streams [first, first+count) of job 0 of `jobs` */
+cudaError_t launch_seed_dump(const KernelParams &P, int64_t first, int64_t count,
+                             uint64_t *x_out, uint32_t *a_out, cudaStream_t stream);
+cudaError_t launch_mwc_draws(const uint64_t *x, const uint32_t *a, int64_t ngen, int64_t n,
+                             float *out, cudaStream_t stream);
+
+} /* namespace mc3d */
+
+#endif
