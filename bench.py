@@ -1,7 +1,9 @@
 """Benchmark: photons/s of the photon-tracking path on B200.
 
-One step = one full simulation of the workload (default: the layered tissue with a
-vessel, 256x256x128 voxels of 0.02 mm, uniform beam, 1e8 photons per GPU).
+Workload: the layered tissue with a vessel, 256x256x128 voxels of 0.02 mm, uniform
+beam, a job of 1e8 photons per GPU.  The job's RNG streams are split into --steps
+equal ranges and one step runs one range, so the K timed steps together are
+exactly the whole job (stream ranges of a job add up bit-for-bit to the job).
 
   value  device throughput: photons / kernel time, inputs resident in HBM, timed
          with CUDA events on the launching stream, L2 flushed between steps.
@@ -47,10 +49,11 @@ FP32_LANES_PER_SM, SFU_LANES_PER_SM = 128, 16
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--photons", type=float, default=1e8, help="photons per GPU per step")
+    ap.add_argument("--photons", type=float, default=1e8, help="photons per GPU per job")
+    ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--math", default="fast", choices=["fast", "exact"])
     ap.add_argument("--ref-photons", type=float, default=1e7)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -172,9 +175,17 @@ def run_ours(args):
     w = layered_vessel(photons=per_gpu * world)
     job = w.jobs[0]
     S = job.num_streams()
-    shard = m.Job(job.geom, job.props, job.photons, job.seed, job.beam, S,
-                  stream_first=rank * S // world,
-                  stream_count=(rank + 1) * S // world - rank * S // world)
+    K = max(1, args.steps)
+
+    def shard(k: int) -> "m.Job":
+        """stream range of step k (of K) owned by this rank"""
+        lo = (k % K) * S // K
+        hi = ((k % K) + 1) * S // K
+        first = lo + rank * (hi - lo) // world
+        last = lo + (rank + 1) * (hi - lo) // world
+        return m.Job(job.geom, job.props, job.photons, job.seed, job.beam, S,
+                     stream_first=first, stream_count=last - first)
+
     g = w.geoms[0]
     pinned = torch.empty(g.tissue.size, dtype=torch.uint8, pin_memory=True)
     pinned.numpy()[:] = g.tissue.reshape(-1)
@@ -184,7 +195,8 @@ def run_ours(args):
     pinned_tab.numpy().view(np.uint32)[:] = table
     table_p = pinned_tab.numpy().view(np.uint32)
 
-    plan = m.Plan([geom], w.props, [shard], table=table_p, math=args.math, device=dev)
+    plans = [m.Plan([geom], w.props, [shard(k)], table=table_p, math=args.math, device=dev)
+             for k in range(K)]
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     nb = g.tissue.shape[1] * g.tissue.shape[2]
@@ -206,9 +218,9 @@ def run_ours(args):
         r.totals = {k: int(v) for k, v in zip(m.TOTAL_FIELDS, a[3 * nb:])}
         return res
 
-    for _ in range(args.warmup):
-        plan.execute(stream.cuda_stream)
-        exchange(plan.read())
+    for k in range(args.warmup):
+        plans[k % K].execute(stream.cuda_stream)
+        exchange(plans[k % K].read())
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
@@ -220,12 +232,12 @@ def run_ours(args):
             torch.cuda.synchronize(dev)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            plan.execute(stream.cuda_stream)
+            plans[k].execute(stream.cuda_stream)
             e1.record(stream)
             e1.synchronize()
             launches += 1
             times.append(e0.elapsed_time(e1) / 1e3)
-            res = exchange(plan.read())
+            res = exchange(plans[k].read())
             steps_tot += res[0].totals["steps"]
             fresnel_tot += res[0].totals["fresnel"]
             photons_tot += res[0].totals["photons"]
@@ -243,27 +255,30 @@ def run_ours(args):
         e2e_times = []
         h2d = g.tissue.size + table_p.nbytes + sum(p.mua.nbytes * 4 for p in w.props)
         d2h = 3 * nb * 8 + 14 * 8
-        for k in range(max(1, args.steps)):
+        e2e_photons = 0
+        for k in range(max(1, min(args.e2e_steps, K))):
             flush.fill_(k & 0xff)
             torch.cuda.synchronize(dev)
             if dist:
                 dist.barrier()
             t0 = time.perf_counter()
-            res = m.run([geom], w.props, [shard], table=table_p, math=args.math, device=dev)
-            exchange(res)
+            res = m.run([geom], w.props, [shard(k)], table=table_p, math=args.math, device=dev)
+            res = exchange(res)
             e2e_times.append(time.perf_counter() - t0)
+            e2e_photons += res[0].totals["photons"]
         te = sum(e2e_times) / len(e2e_times)
         if dist:
             tt = torch.tensor([te], dtype=torch.float64, device=dev)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             te = float(tt.item())
-        e2e = {"value": photons_step / te, "unit": "photons/s", "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": e2e_photons / len(e2e_times) / te, "unit": "photons/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": te * 1e3,
                "timing": "host clock around the synchronous mc3d_run call (plan, upload, "
                          "kernel, read-back), max over ranks"}
 
     if rank != 0:
-        plan.close()
+        for pl in plans:
+            pl.close()
         if dist:
             dist.barrier()
             dist.destroy_process_group()
@@ -285,15 +300,17 @@ def run_ours(args):
             traffic = json.loads(tp.read_text()).get("bytes_per_launch")
         except Exception:
             traffic = None
-    block, grid, smem = plan.shape()
+    block, grid, smem = plans[0].shape()
     line = {
         "metric": "photons/s (layered tissue + vessel, 256x256x128, uniform beam, 1 B200)",
         "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+u64",
         "data": "synthetic (seeded layered-tissue geometry, reference input formats)",
-        "config": {"workload": w.name, "photons_per_step": int(photons_step),
-                   "photons_per_gpu": per_gpu, "voxels": list(g.shape), "voxel_mm": g.dx,
+        "config": {"workload": w.name, "photons_per_job": int(job.photons),
+                   "photons_per_step": int(photons_step),
+                   "step": f"1/{K} of the job's RNG streams; the {K} timed steps are the "
+                           "whole job", "voxels": list(g.shape), "voxel_mm": g.dx,
                    "beam": "uniform", "math": args.math, "streams": S,
                    "launch": {"block": block, "grid": grid, "smem": smem},
                    "l2": "flushed between steps (256 MB write)",
@@ -313,7 +330,8 @@ def run_ours(args):
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
-    plan.close()
+    for pl in plans:
+        pl.close()
     print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -1,0 +1,57 @@
+"""The gpu-mc command: the reference's argument handling, messages and output files
+(src/mc3d_main.cu:15-98)."""
+from __future__ import annotations
+
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, has_gpu
+from ymc3d_b200.workloads import read_drs_file, write_geometry_file, write_optprops_file
+
+CLI = ROOT / "ymc3d_b200" / "gpu-mc"
+
+
+def run(args, cwd):
+    return subprocess.run([str(CLI)] + [str(a) for a in args], cwd=cwd, capture_output=True,
+                          text=True, timeout=600)
+
+
+def inputs(tmp_path, n=16, rows=((0.1, 10.0, 0.9, 1.4),)):
+    write_geometry_file(tmp_path / "geom.bin", np.ones((n, n, n), np.uint8), 0.1, 0.1, 0.1)
+    write_optprops_file(tmp_path / "props.bid", rows)
+    return tmp_path / "geom.bin", tmp_path / "props.bid"
+
+
+def test_usage(engine, tmp_path):
+    r = run(["a", "b"], tmp_path)
+    assert r.returncode == 1 and "Usage:" in r.stderr
+
+
+def test_missing_inputs(engine, tmp_path):
+    g, p = inputs(tmp_path)
+    r = run([tmp_path / "nope.bin", p, "dummy", "out"], tmp_path)
+    assert r.returncode == 1 and "was not opened" in r.stderr
+
+
+def test_missing_table_exits_like_reference(engine, tmp_path):
+    g, p = inputs(tmp_path)
+    r = run([g, p, "dummy", "out"], tmp_path)
+    assert r.returncode == 1 and "Couldn't find safeprimes_base32.txt." in r.stderr
+    assert "#mua (mm-1), mus (mm-1), g, n." in r.stdout  # printed before the run
+
+
+@pytest.mark.gpu
+def test_cli_run_matches_library(engine, tmp_path, table):
+    g, p = inputs(tmp_path)
+    engine.write_safeprimes(tmp_path / "safeprimes_base32.txt", table[:230401])
+    (tmp_path / "params.txt").write_text("photons = 20000\nseed = 4242\nbeam = pencil\n")
+    r = run([g, p, "params.txt", "out"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "seed: 4242" in r.stderr and "Total diffuse reflectance is" in r.stderr
+    assert (tmp_path / "out_simparam.dat").read_text() == "20000 #num_photons\n"
+    drs, dx, dy = read_drs_file(tmp_path / "out_drs.bin")
+    res = engine.run([engine.geometry_read_from_file(g)], [engine.opticalprops_read_from_file(p)],
+                     [engine.Job(0, 0, 20000, 4242, "pencil")], table=table[:230401])[0]
+    assert np.array_equal(drs, res.drs.astype(np.float64) / engine.WEIGHT_SCALE / 20000)

@@ -31,7 +31,7 @@ UNITS = {
     "mc3d_kernel_exact.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
                              "-Xptxas", "-v"],
     "mc3d_seed.cu": ["-fmad=false"],
-    "mc3d_api.cu": ["-fmad=false"],
+    "mc3d_api.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"],
 }
 CXX_UNITS = ["mc3d_safeprimes.cpp", "mc3d_io.cpp"]
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-pthread", "-ffp-contract=off", "-I", str(CSRC),

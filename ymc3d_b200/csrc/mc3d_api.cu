@@ -221,7 +221,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
                 !std::isfinite(p.n[t]))
                 return fail(MC3D_ERR_PROPS, "optical set %d: tissue %d not finite", i, t);
         props_offset[i] = entries;
-        entries += p.num_tissue_types;
+        entries += 3 * p.num_tissue_types;
     }
     if ((int64_t)entries * 16 > kMaxSharedTable)
         return fail(MC3D_ERR_CAPACITY, "optical tables need %d bytes of shared memory (max %d)",
@@ -335,6 +335,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         d.dx = (float)g.dx; d.dy = (float)g.dy; d.dz = (float)g.dz;
         /* geometry->length_x = sample_dx*num_x in float (src/mc3d_io.cu:143-145) */
         d.Lx = d.dx * g.nx; d.Ly = d.dy * g.ny; d.Lz = d.dz * g.nz;
+        d.rdx = 1.0f / d.dx; d.rdy = 1.0f / d.dy; d.rdz = 1.0f / d.dz;
         d.tissue = p->d_grids[i];
     }
     PLAN_TRY(cudaMalloc(&p->d_geoms, sizeof(GeomDev) * ngeoms));
@@ -342,11 +343,21 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
                              cudaMemcpyHostToDevice, p->stream));
 
     /* ---- optical tables */
+    /* three float4 per tissue; every derived value is the float the reference
+     * computes per step (IEEE, no contraction: this file is built with
+     * -ffp-contract=off), except 1/mu_t, which only the fast kernel reads */
     std::vector<float4> tab(entries);
     for (int i = 0; i < nprops; i++)
-        for (int t = 0; t < props[i].num_tissue_types; t++)
-            tab[props_offset[i] + t] =
-                make_float4(props[i].mua[t], props[i].mus[t], props[i].g[t], props[i].n[t]);
+        for (int t = 0; t < props[i].num_tissue_types; t++) {
+            float mua = props[i].mua[t], mus = props[i].mus[t], g = props[i].g[t];
+            volatile float mut = mua + mus;
+            volatile float frac = mua / mut, rmut = 1.0f / mut, g2 = g * g, twog = 2 * g;
+            volatile float inv2g = 1.0f / twog;
+            float4 *e = &tab[props_offset[i] + 3 * t];
+            e[0] = make_float4(mua, mus, g, props[i].n[t]);
+            e[1] = make_float4(mut, frac, rmut, inv2g);
+            e[2] = make_float4(1 - g2, 1 - g, twog, 1 + g2);
+        }
     PLAN_TRY(cudaMalloc(&p->d_props, sizeof(float4) * entries));
     PLAN_TRY(cudaMemcpyAsync(p->d_props, tab.data(), sizeof(float4) * entries,
                              cudaMemcpyHostToDevice, p->stream));

@@ -20,6 +20,8 @@ struct GeomDev {
     int nx, ny, nz, pad;
     float dx, dy, dz;      /* voxel size, float as in geometry_t (src/mc3d_types.h:38-43) */
     float Lx, Ly, Lz;      /* voxel size * count, computed in float */
+    float rdx, rdy, rdz;   /* 1 / voxel size (fast math only) */
+    float pad2;
     const uint8_t *tissue; /* nz*ny*nx, x fastest; 0 = air */
 };
 
@@ -61,7 +63,7 @@ struct PhotonRecord {
 struct KernelParams {
     const JobDev *jobs;
     const GeomDev *geoms;
-    const float4 *props_table; /* (mua, mus, g, n) per tissue, all sets back to back */
+    const float4 *props_table; /* 3 float4 per tissue (see photon_step), sets back to back */
     const uint32_t *multipliers; /* safe-prime table, entry 0 = seeding multiplier */
     const RejectionDev *rejections;
     unsigned long long *drs;    /* sum Q(W) of reflected photons per surface bin */

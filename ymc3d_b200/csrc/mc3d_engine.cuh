@@ -34,7 +34,10 @@ namespace mc3d {
 
 /* ---------------------------------------------------------------- math policies */
 struct MathExact {
+    static constexpr bool kFast = false;
     static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    /* a / b where the caller also holds r = 1/b: the exact policy divides */
+    static __device__ __forceinline__ float div_r(float a, float b, float) { return a / b; }
     static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
     static __device__ __forceinline__ float rsqrt(float x) { return 1.0f / sqrtf(x); }
     static __device__ __forceinline__ float log(float x) { return mc3d_xm_logf(x); }
@@ -49,15 +52,21 @@ struct MathExact {
 /* Compiled only in a translation unit built with -use_fast_math, where the
  * operators and functions below map to the approximate hardware paths. */
 struct MathFast {
+    static constexpr bool kFast = true;
     static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    static __device__ __forceinline__ float div_r(float a, float, float r) { return a * r; }
     static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
     static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
     static __device__ __forceinline__ float log(float x) { return logf(x); }
     static __device__ __forceinline__ float acos(float x) { return acosf(x); }
     static __device__ __forceinline__ float sin(float x) { return sinf(x); }
+    /* sin/cos(pi x) for x in [0, 2): the SFU's sin/cos on pi (x - 1) in [-pi, pi) */
     static __device__ __forceinline__ void sincospi(float x, float *s, float *c)
     {
-        sincospif(x, s, c);
+        float sn, cs;
+        __sincosf(3.14159265358979f * (x - 1.0f), &sn, &cs);
+        *s = -sn;
+        *c = -cs;
     }
 };
 
@@ -77,6 +86,7 @@ struct MathFast {
 #define MC3D_UZ_THRESH_LE_F 0x1.fffeb0p-1f
 #define MC3D_NUM_PHOTON_STEPS 45
 #define MC3D_TISSUE_AIR 0
+#define MC3D_TAB_STRIDE 3 /* float4 per tissue in the optical table */
 
 /* fixed-point weight, 2^-32 resolution */
 static __device__ __forceinline__ uint64_t qw(float w)
@@ -86,9 +96,9 @@ static __device__ __forceinline__ uint64_t qw(float w)
 
 /* src/mc3d_gpu.cu:53-63 */
 template <class M>
-static __device__ __forceinline__ int grid_coord(float x, float ux, float d)
+static __device__ __forceinline__ int grid_coord(float x, float ux, float d, float rd)
 {
-    int i = (int)floorf(M::div(x, d));
+    int i = (int)floorf(M::div_r(x, d, rd));
     i += (x == (float)(int)((unsigned)i + 1u) * d);
     float bmin = (float)i * d;
     i = ((x > bmin) || ((x == bmin) && (ux >= 0))) ? i : i - 1;
@@ -140,10 +150,22 @@ struct Photon {
     int i, j, k, tissue;
 };
 
-/* Per-photon weight bookkeeping (fixed point) for the conservation identity
- *   Q(W0) = absorbed + exit + rr_killed - rr_created + lost. */
-struct PhotonBook {
-    uint64_t killed, created;
+/* Per-thread tallies live in shared memory, one column per thread, so that the
+ * step loop keeps only the photon in registers.  They are touched when a photon
+ * ends or at a roulette event, and flushed to the job's totals when the thread
+ * moves to another stream.  Slot order is mc3d_totals (include/mc3d.h). */
+enum {
+    T_PHOTONS = 0, T_STEPS, T_W_LAUNCHED, T_R_IN, T_R_OUT, T_T_IN, T_T_OUT, T_ABSORBED,
+    T_RR_KILLED, T_RR_CREATED, T_LOST, T_CAPPED, T_QUICKFIX, T_FRESNEL
+};
+#define MC3D_MAX_BLOCK 256
+
+struct Acc {
+    unsigned long long *col; /* sh_acc + threadIdx.x; slot t at col[t * MC3D_MAX_BLOCK] */
+    __device__ __forceinline__ unsigned long long &operator[](int t) const
+    {
+        return col[t * MC3D_MAX_BLOCK];
+    }
 };
 
 /* One step of src/mc3d_gpu.cu:175-340 for a live photon.  Returns true when the
@@ -151,30 +173,35 @@ struct PhotonBook {
 template <class M>
 static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float4 *tab,
                                                    Photon &p, uint64_t &rx, uint32_t ra,
-                                                   PhotonBook &bk, float *db_out,
+                                                   const Acc &acc, float *db_out,
                                                    uint32_t *fresnel_count)
 {
-    const float4 cur = tab[p.tissue]; /* mua, mus, g, n */
-    float ni = cur.w;
+    /* per tissue: (mua, mus, g, n), (mu_t, mua/mu_t, 1/mu_t, 1/(2g)),
+     * (1-g^2, 1-g, 2g, 1+g^2) -- each the float the reference computes per step */
+    const float4 t0 = tab[MC3D_TAB_STRIDE * p.tissue];
+    const float4 t1 = tab[MC3D_TAB_STRIDE * p.tissue + 1];
+    const float4 t2 = tab[MC3D_TAB_STRIDE * p.tissue + 2];
+    float ni = t0.w;
     float nt = ni;
-    float mu_a = cur.x, mu_s = cur.y, gg = cur.z;
-    float mu_t = mu_a + mu_s;
+    float mu_a = t0.x;
+    float mu_t = t1.x;
+    (void)mu_a;
 
     float newx = p.x, newy = p.y, newz = p.z;
     float db = intersection<M>(g, p.i, p.j, p.k, &newx, p.ux, &newy, p.uy, &newz, p.uz);
 
     bool hit = db * mu_t <= p.s;
     float ds = hit ? db * mu_t : p.s;
-    newx = hit ? newx : p.x + M::div(p.ux * ds, mu_t);
-    newy = hit ? newy : p.y + M::div(p.uy * ds, mu_t);
-    newz = hit ? newz : p.z + M::div(p.uz * ds, mu_t);
+    newx = hit ? newx : p.x + M::div_r(p.ux * ds, mu_t, t1.z);
+    newy = hit ? newy : p.y + M::div_r(p.uy * ds, mu_t, t1.z);
+    newz = hit ? newz : p.z + M::div_r(p.uz * ds, mu_t, t1.z);
     float s = p.s - ds;
 
-    int nexti = grid_coord<M>(newx, p.ux, g.dx);
-    int nextj = grid_coord<M>(newy, p.uy, g.dy);
-    int nextk = grid_coord<M>(newz, p.uz, g.dz);
+    int nexti = grid_coord<M>(newx, p.ux, g.dx, g.rdx);
+    int nextj = grid_coord<M>(newy, p.uy, g.dy, g.rdy);
+    int nextk = grid_coord<M>(newz, p.uz, g.dz, g.rdz);
     int next_tissue = tissue_at(g, nexti, nextj, nextk, newz, p.uz);
-    nt = tab[next_tissue].w;
+    nt = tab[MC3D_TAB_STRIDE * next_tissue].w;
 
     float tr_ux = p.ux, tr_uy = p.uy, tr_uz = p.uz;
     bool refl = false;
@@ -208,7 +235,7 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
 
     /* absorption, src/mc3d_gpu.cu:262-263 */
     float W = p.W;
-    float dW = (mu_t > 0) ? M::div(mu_a, mu_t) * W : 0;
+    float dW = (mu_t > 0) ? t1.y * W : 0;
     W = W - dW * (float)(!hit);
 
     /* russian roulette, src/mc3d_gpu.cu:275-277 */
@@ -216,14 +243,23 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     bool roulette = (W <= MC3D_W_THRESHOLD_LE_F) && (!hit) && (mu_t != 0);
     if (roulette) {
         float newW = (eps < MC3D_SURVIVAL_LT_F) ? (float)((double)W / MC3D_SURVIVAL_CHANCE) : 0.0f;
-        if (newW == 0.0f) bk.killed += qw(W);
-        else bk.created += qw(newW) - qw(W);
+        /* absorbed weight is booked at the photon's end as Q(W0) - Q(W_end) - lost;
+         * a roulette event moves its share from there to the roulette tallies */
+        if (newW == 0.0f) {
+            uint64_t k = qw(W);
+            acc[T_RR_KILLED] += k;
+            acc[T_ABSORBED] -= k;
+        } else {
+            uint64_t c = qw(newW) - qw(W);
+            acc[T_RR_CREATED] += c;
+            acc[T_ABSORBED] += c;
+        }
         W = newW;
     }
 
     /* Henyey-Greenstein, src/mc3d_gpu.cu:282-294 */
-    float costheta = M::div(1 - gg * gg, 1 - gg + 2 * gg * mc3d_rand_oc(&rx, ra));
-    costheta = M::div(1.0f, 2 * gg) * (1 + gg * gg - costheta * costheta);
+    float costheta = M::div(t2.x, t2.y + t2.z * mc3d_rand_oc(&rx, ra));
+    costheta = t1.w * (t2.w - costheta * costheta);
     float sintheta = M::sqrt(1 - costheta * costheta);
     float phi_divpi = 2 * mc3d_rand_co(&rx, ra);
     float cosphi, sinphi;
@@ -282,9 +318,9 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
 template <class M>
 static __device__ __forceinline__ void derive_cell(const GeomDev &g, Photon &p)
 {
-    p.i = grid_coord<M>(p.x, p.ux, g.dx);
-    p.j = grid_coord<M>(p.y, p.uy, g.dy);
-    p.k = grid_coord<M>(p.z, p.uz, g.dz);
+    p.i = grid_coord<M>(p.x, p.ux, g.dx, g.rdx);
+    p.j = grid_coord<M>(p.y, p.uy, g.dy, g.rdy);
+    p.k = grid_coord<M>(p.z, p.uz, g.dz, g.rdz);
     p.tissue = tissue_at(g, p.i, p.j, p.k, p.z, p.uz);
 }
 
@@ -323,35 +359,20 @@ static __device__ __forceinline__ float masked_steps(const GeomDev &g, Photon &p
 }
 
 /* --------------------------------------------------------------- kernel body */
-struct ThreadAcc {
-    uint64_t photons, steps, w_launched, r_in, r_out, t_in, t_out, absorbed;
-    uint64_t rr_killed, rr_created, lost, capped, quickfix, fresnel;
-};
-
-static __device__ __forceinline__ void acc_clear(ThreadAcc &a)
+static __device__ __forceinline__ void acc_clear(const Acc &a)
 {
-    a.photons = a.steps = a.w_launched = a.r_in = a.r_out = a.t_in = a.t_out = a.absorbed = 0;
-    a.rr_killed = a.rr_created = a.lost = a.capped = a.quickfix = a.fresnel = 0;
+#pragma unroll
+    for (int t = 0; t < MC3D_NUM_TOTALS; t++) a[t] = 0;
 }
 
-static __device__ __forceinline__ void acc_flush(ThreadAcc &a, unsigned long long *tot)
+static __device__ __forceinline__ void acc_flush(const Acc &a, unsigned long long *tot)
 {
-    if (a.photons == 0 && a.steps == 0) return;
-    atomicAdd(tot + 0, (unsigned long long)a.photons);
-    atomicAdd(tot + 1, (unsigned long long)a.steps);
-    atomicAdd(tot + 2, (unsigned long long)a.w_launched);
-    atomicAdd(tot + 3, (unsigned long long)a.r_in);
-    if (a.r_out) atomicAdd(tot + 4, (unsigned long long)a.r_out);
-    if (a.t_in) atomicAdd(tot + 5, (unsigned long long)a.t_in);
-    if (a.t_out) atomicAdd(tot + 6, (unsigned long long)a.t_out);
-    atomicAdd(tot + 7, (unsigned long long)a.absorbed);
-    if (a.rr_killed) atomicAdd(tot + 8, (unsigned long long)a.rr_killed);
-    if (a.rr_created) atomicAdd(tot + 9, (unsigned long long)a.rr_created);
-    if (a.lost) atomicAdd(tot + 10, (unsigned long long)a.lost);
-    if (a.capped) atomicAdd(tot + 11, (unsigned long long)a.capped);
-    if (a.quickfix) atomicAdd(tot + 12, (unsigned long long)a.quickfix);
-    if (a.fresnel) atomicAdd(tot + 13, (unsigned long long)a.fresnel);
-    acc_clear(a);
+#pragma unroll
+    for (int t = 0; t < MC3D_NUM_TOTALS; t++) {
+        unsigned long long v = a[t];
+        if (v) atomicAdd(tot + t, v);
+        a[t] = 0;
+    }
 }
 
 /* job owning global stream index gs (binary search over the stream prefix) */
@@ -390,21 +411,19 @@ template <class M>
 __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
 {
     extern __shared__ float4 sh_tab[];
+    __shared__ unsigned long long sh_acc[MC3D_NUM_TOTALS * MC3D_MAX_BLOCK];
     for (int t = threadIdx.x; t < P.props_entries; t += blockDim.x) sh_tab[t] = P.props_table[t];
+    const Acc acc{sh_acc + threadIdx.x};
+    acc_clear(acc);
     __syncthreads();
 
-    ThreadAcc acc;
-    acc_clear(acc);
     int job = -1;
-    unsigned long long *job_tot = nullptr;
     GeomDev g;
     const float4 *tab = sh_tab;
-    JobDev jb;
-    int64_t left = 0, local = 0, kphot = 0;
+    int64_t left = 0, local = 0;
     uint64_t rx = 0;
     uint32_t ra = 1;
     Photon p;
-    PhotonBook bk;
     bool alive = false;
     int chunk = 0;
     uint32_t psteps = 0;
@@ -415,26 +434,22 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
     for (;;) {
         if (!alive) {
             if (left == 0) {
-                acc.fresnel += fresnel;
-                fresnel = 0;
-                if (job_tot) acc_flush(acc, job_tot);
+                if (job >= 0) acc_flush(acc, P.totals + (int64_t)job * MC3D_NUM_TOTALS);
                 if (P.cancel && *((volatile const int *)P.cancel)) break;
                 int64_t gs = (int64_t)atomicAdd((unsigned long long *)P.work_counter, 1ull);
                 if (gs >= P.total_streams) break;
                 job = find_job(P.jobs, P.njobs, gs);
-                jb = P.jobs[job];
+                const JobDev &jb = P.jobs[job];
                 g = P.geoms[jb.geom];
                 tab = sh_tab + jb.props_offset;
-                job_tot = P.totals + (int64_t)job * MC3D_NUM_TOTALS;
                 local = gs - jb.stream_base + jb.stream_first;
                 left = jb.per_stream + (local < jb.remainder ? 1 : 0);
-                kphot = 0;
                 ra = P.multipliers[1 + (local % (P.num_multipliers - 1))];
                 rx = stream_seed(P, jb, local, ra);
                 if (left == 0) continue;
             }
             /* photontrack_reinitialize, src/mc3d_gpu.cu:74-111 */
-            if (jb.beam == 0) {
+            if (P.jobs[job].beam == 0) {
                 p.x = g.Lx * mc3d_rand_co(&rx, ra);
                 p.y = g.Ly * mc3d_rand_co(&rx, ra);
             } else {
@@ -444,22 +459,22 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
             p.z = 0;
             p.ux = 0; p.uy = 0; p.uz = 1;
             /* specular reflection from air into tissue type 1 (src/mc3d_gpu.cu:67-70, 500) */
-            float rsp = M::div(tab[MC3D_TISSUE_AIR].w - tab[1].w, tab[MC3D_TISSUE_AIR].w + tab[1].w);
+            const float n0 = tab[MC3D_TAB_STRIDE * MC3D_TISSUE_AIR].w, n1 = tab[MC3D_TAB_STRIDE].w;
+            float rsp = M::div(n0 - n1, n0 + n1);
             rsp = rsp * rsp;
             p.W = 1.0f - rsp;
             qw0 = qw(p.W);
             p.s = -M::log(mc3d_rand_oc(&rx, ra));
             derive_cell<M>(g, p);
-            bk.killed = 0; bk.created = 0;
             chunk = 0;
             psteps = 0;
+            fresnel = 0;
             alive = true;
             left--;
-            acc.w_launched += qw0;
         }
 
         float db;
-        bool froze = photon_step<M>(g, tab, p, rx, ra, bk, &db, &fresnel);
+        bool froze = photon_step<M>(g, tab, p, rx, ra, acc, &db, &fresnel);
         chunk++;
         psteps++;
 
@@ -468,51 +483,48 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
         if (froze) {
             db = masked_steps<M>(g, p, MC3D_NUM_PHOTON_STEPS - chunk, db);
             float w_before = p.W;
-            if (quickfix(p, db)) { acc.quickfix++; lost = qw(w_before); }
+            if (quickfix(p, db)) { acc[T_QUICKFIX]++; lost = qw(w_before); }
             done = true;
         } else if (chunk == MC3D_NUM_PHOTON_STEPS) {
             float w_before = p.W;
-            if (quickfix(p, db)) { acc.quickfix++; lost = qw(w_before); done = true; }
+            if (quickfix(p, db)) { acc[T_QUICKFIX]++; lost = qw(w_before); done = true; }
             else { derive_cell<M>(g, p); chunk = 0; }
         }
         if (!done && (int64_t)psteps >= max_steps) {
             lost = qw(p.W);
             p.W = 0;
-            acc.capped++;
+            acc[T_CAPPED]++;
             done = true;
         }
         if (done) {
             /* photon_detector, src/mc3d_photons.cu:151-171 */
-            int ix = grid_coord<M>(p.x, p.ux, g.dx);
-            int iy = grid_coord<M>(p.y, p.uy, g.dy);
+            const JobDev &jb = P.jobs[job];
+            int ix = grid_coord<M>(p.x, p.ux, g.dx, g.rdx);
+            int iy = grid_coord<M>(p.y, p.uy, g.dy, g.rdy);
             bool inside = (ix >= 0) && (iy >= 0) && (ix < g.nx) && (iy < g.ny);
             uint64_t q = qw(p.W);
             int64_t bin = jb.bin_offset + (int64_t)iy * g.nx + ix;
+            int slot;
             if (p.z <= 0) {
-                if (inside) {
-                    if (q) {
-                        atomicAdd(P.drs + bin, (unsigned long long)q);
-                        atomicAdd(P.drs_sq + bin, (unsigned long long)qw(p.W * p.W));
-                    }
-                    acc.r_in += q;
-                } else {
-                    acc.r_out += q;
+                slot = inside ? T_R_IN : T_R_OUT;
+                if (inside && q) {
+                    atomicAdd(P.drs + bin, (unsigned long long)q);
+                    atomicAdd(P.drs_sq + bin, (unsigned long long)qw(p.W * p.W));
                 }
             } else {
-                if (inside) {
-                    if (q) atomicAdd(P.trans + bin, (unsigned long long)q);
-                    acc.t_in += q;
-                } else {
-                    acc.t_out += q;
-                }
+                slot = inside ? T_T_IN : T_T_OUT;
+                if (inside && q) atomicAdd(P.trans + bin, (unsigned long long)q);
             }
-            acc.absorbed += qw0 - q - bk.killed + bk.created - lost;
-            acc.rr_killed += bk.killed;
-            acc.rr_created += bk.created;
-            acc.lost += lost;
-            acc.photons++;
-            acc.steps += psteps;
+            acc[slot] += q;
+            acc[T_W_LAUNCHED] += qw0;
+            acc[T_ABSORBED] += qw0 - q - lost;
+            acc[T_LOST] += lost;
+            acc[T_PHOTONS] += 1;
+            acc[T_STEPS] += psteps;
+            acc[T_FRESNEL] += fresnel;
             if (P.photon_log) {
+                int64_t nstream = jb.per_stream + (local < jb.remainder ? 1 : 0);
+                int64_t kphot = nstream - left - 1;
                 int64_t pid = jb.photon_base + local + kphot * jb.streams;
                 PhotonRecord r;
                 r.x = p.x; r.y = p.y; r.z = p.z;
@@ -523,12 +535,10 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
                 r.rng = rx;
                 P.photon_log[pid] = r;
             }
-            kphot++;
             alive = false;
         }
     }
-    acc.fresnel += fresnel;
-    if (job_tot) acc_flush(acc, job_tot);
+    if (job >= 0) acc_flush(acc, P.totals + (int64_t)job * MC3D_NUM_TOTALS);
 }
 
 } /* namespace mc3d */

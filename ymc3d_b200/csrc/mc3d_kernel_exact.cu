@@ -9,7 +9,7 @@
 
 namespace mc3d {
 
-__global__ void __launch_bounds__(256) photon_kernel_exact(const __grid_constant__ KernelParams P)
+__global__ void __launch_bounds__(256, 3) photon_kernel_exact(const __grid_constant__ KernelParams P)
 {
     photon_kernel_body<MathExact>(P);
 }
