@@ -49,7 +49,7 @@ FP32_LANES_PER_SM, SFU_LANES_PER_SM = 128, 16
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--photons", type=float, default=1e8, help="photons per GPU per job")
@@ -197,7 +197,8 @@ def run_ours(args):
 
     plans = [m.Plan([geom], w.props, [shard(k)], table=table_p, math=args.math, device=dev)
              for k in range(K)]
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # a real stream handle (the legacy default stream is 0)
+    torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     nb = g.tissue.shape[1] * g.tissue.shape[2]
 

@@ -107,6 +107,9 @@ typedef struct {
     uint64_t *drs;     /* sum Q(W) of reflected photons per surface bin */
     uint64_t *drs_sq;  /* sum Q(W^2) per bin, for the per-bin variance */
     uint64_t *trans;   /* sum Q(W) of photons frozen below the surface */
+    uint64_t *absorption; /* nz*ny*nx: sum Q(W_before) - Q(W_after) of every absorption in
+                             the voxel (clamped into the grid, as the reference's disabled
+                             tally, src/mc3d_gpu.cu:265-272); needs options.absorption_map */
     mc3d_totals totals;
 } mc3d_out;
 
@@ -123,6 +126,8 @@ typedef struct {
     int32_t math;           /* enum mc3d_math */
     int32_t block;          /* threads per block, 0 = tuned */
     int32_t blocks_per_sm;  /* 0 = as many as fit */
+    int32_t absorption_map; /* 1: tally absorbed weight per voxel (sum over voxels = absorbed) */
+    int32_t reserved;
     int64_t max_steps;      /* per-photon step cap, 0 = 2^24 */
     mc3d_photon_record *photon_log; /* host, sum of photons over jobs, or NULL */
     volatile int32_t *cancel;       /* optional host flag, read when a stream starts */

@@ -54,7 +54,7 @@ def lib():
         h.orc_run.restype = C.c_int
         h.orc_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int,
                               C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
-                              C.c_void_p, C.c_void_p]
+                              C.c_void_p, C.c_void_p, C.c_void_p]
         for f in ("orc_logf", "orc_acosf", "orc_sinf"):
             getattr(h, f).restype = C.c_float
             getattr(h, f).argtypes = [C.c_float]
@@ -86,7 +86,8 @@ def rand_co(x: int, a: int, n: int) -> np.ndarray:
 
 def run(tissue: np.ndarray, dx: float, dy: float, dz: float, mua, mus, g, n, photons: int,
         streams: int, seed: int, table: np.ndarray, beam: int = 0, threads: int = 0,
-        first: int = 0, count: int = -1, max_steps: int = 0, photon_log: bool = False):
+        first: int = 0, count: int = -1, max_steps: int = 0, photon_log: bool = False,
+        absorption_map: bool = False):
     """Simulate streams [first, first+count) of a job; returns dict with drs, drs_sq,
     trans ([ny, nx] uint64), totals and the optional per-photon log."""
     tissue = np.ascontiguousarray(tissue, np.uint8)
@@ -101,12 +102,14 @@ def run(tissue: np.ndarray, dx: float, dy: float, dz: float, mua, mus, g, n, pho
     trans = np.zeros((ny, nx), np.uint64)
     tot = np.zeros(len(TOTAL_FIELDS), np.uint64)
     log = np.zeros(max(photons, 1), REC_DTYPE) if photon_log else None
+    amap = np.zeros((nz, ny, nx), np.uint64) if absorption_map else None
     st = lib().orc_run(C.byref(geom), C.byref(props), C.byref(job), table.ctypes.data,
                        len(table), threads, first, count, drs.ctypes.data, drs_sq.ctypes.data,
                        trans.ctypes.data, tot.ctypes.data,
-                       None if log is None else log.ctypes.data)
+                       None if log is None else log.ctypes.data,
+                       None if amap is None else amap.ctypes.data)
     if st:
         raise ValueError(f"orc_run status {st}")
     return {"drs": drs, "drs_sq": drs_sq, "trans": trans,
             "totals": {k: int(v) for k, v in zip(TOTAL_FIELDS, tot)},
-            "photon_log": None if log is None else log[:photons]}
+            "photon_log": None if log is None else log[:photons], "absorption": amap}

@@ -200,7 +200,8 @@ typedef struct {
 
 /* photontrack_step body for one live photon; returns 1 on freeze */
 static int orc_step(const orc_g *G, const orc_tab *P, orc_ph *p, uint64_t *rx, uint32_t ra,
-                    uint64_t *killed, uint64_t *created, float *db_out, uint64_t *fresnel)
+                    uint64_t *killed, uint64_t *created, float *db_out, uint64_t *fresnel,
+                    uint64_t *amap)
 {
     int tissue_type = p->tissue;
     float ni = P->n[tissue_type];
@@ -262,6 +263,15 @@ static int orc_step(const orc_g *G, const orc_tab *P, orc_ph *p, uint64_t *rx, u
     float W = p->W;
     float dW = (mu_t > 0) ? mu_a / mu_t * W : 0;
     W = W - dW * (float)(!hit_boundary);
+    if (amap && (!hit_boundary) && (mu_t > 0)) {
+        /* the reference's disabled absorption tally (src/mc3d_gpu.cu:265-272) */
+        int abs_i = orc_clampi(p->i, 0, G->nx - 1);
+        int abs_j = orc_clampi(p->j, 0, G->ny - 1);
+        int abs_k = orc_clampi(p->k, 0, G->nz - 1);
+        uint64_t dq = orc_q(p->W) - orc_q(W);
+#pragma omp atomic
+        amap[((int64_t)abs_k * G->ny + abs_j) * G->nx + abs_i] += dq;
+    }
 
     epsilon = orc_rand_co1(rx, ra);
     float newW = (epsilon < ORC_SURVIVAL_CHANCE) ? (float)(W / ORC_SURVIVAL_CHANCE) : 0;
@@ -353,7 +363,7 @@ typedef struct {
 
 /* one photon of a slot, from reinitialisation to the detector */
 static void orc_photon(const orc_g *G, const orc_tab *P, int beam, int64_t max_steps, uint64_t *rx,
-                       uint32_t ra, orc_acc *acc, orc_rec *rec)
+                       uint32_t ra, orc_acc *acc, orc_rec *rec, uint64_t *amap)
 {
     orc_ph p;
     if (beam == 0) {
@@ -378,7 +388,7 @@ static void orc_photon(const orc_g *G, const orc_tab *P, int beam, int64_t max_s
     int64_t steps = 0;
     for (;;) {
         float db;
-        int froze = orc_step(G, P, &p, rx, ra, &killed, &created, &db, &fresnel);
+        int froze = orc_step(G, P, &p, rx, ra, &killed, &created, &db, &fresnel, amap);
         chunk++;
         steps++;
         int done = 0;
@@ -447,10 +457,12 @@ static void orc_photon(const orc_g *G, const orc_tab *P, int beam, int64_t max_s
 
 /* Simulate streams [first, first + count) of a job (count < 0: to the end).
  * Bin arrays are nx*ny and accumulated into; totals[14] likewise (order of
- * mc3d_totals).  log, if given, has one record per photon of the whole job. */
+ * mc3d_totals).  log, if given, has one record per photon of the whole job; amap, if
+ * given, is nz*ny*nx and accumulates the absorbed fixed-point weight per voxel. */
 int orc_run(const orc_geom *geom, const orc_props *props, const orc_job *job,
             const uint32_t *table, int64_t table_len, int nthreads, int64_t first, int64_t count,
-            uint64_t *drs, uint64_t *drs_sq, uint64_t *trans, uint64_t *totals, orc_rec *log)
+            uint64_t *drs, uint64_t *drs_sq, uint64_t *trans, uint64_t *totals, orc_rec *log,
+            uint64_t *amap)
 {
     if (job->streams <= 0 || props->ntypes < 2) return 4;
     int64_t S = job->streams;
@@ -491,7 +503,7 @@ int orc_run(const orc_geom *geom, const orc_props *props, const orc_job *job,
             int64_t np = per + (i < rem ? 1 : 0);
             for (int64_t k = 0; k < np; k++) {
                 orc_rec *rec = log ? &log[i + k * S] : NULL;
-                orc_photon(&G, &P, job->beam, max_steps, &rx, ra, &acc, rec);
+                orc_photon(&G, &P, job->beam, max_steps, &rx, ra, &acc, rec, amap);
             }
         }
 #pragma omp critical

@@ -9,11 +9,12 @@ import ymc3d_b200 as m
 
 
 def oracle_job(geom: m.Geometry, props: m.OpticalProps, job: m.Job, table, threads=0,
-               photon_log=False, first=0, count=-1, max_steps=0):
+               photon_log=False, first=0, count=-1, max_steps=0, absorption_map=False):
     return oracle.run(geom.tissue, geom.dx, geom.dy, geom.dz, props.mua, props.mus, props.g,
                       props.n, int(job.photons), job.num_streams(), int(job.seed), table,
                       beam=m.BEAMS[job.beam], threads=threads, first=first, count=count,
-                      max_steps=max_steps, photon_log=photon_log)
+                      max_steps=max_steps, photon_log=photon_log,
+                      absorption_map=absorption_map)
 
 
 def residual(t: dict) -> int:

@@ -55,3 +55,23 @@ def test_cli_run_matches_library(engine, tmp_path, table):
     res = engine.run([engine.geometry_read_from_file(g)], [engine.opticalprops_read_from_file(p)],
                      [engine.Job(0, 0, 20000, 4242, "pencil")], table=table[:230401])[0]
     assert np.array_equal(drs, res.drs.astype(np.float64) / engine.WEIGHT_SCALE / 20000)
+
+
+@pytest.mark.gpu
+def test_cli_absorption_and_transmission_maps(engine, tmp_path, table):
+    write_geometry_file(tmp_path / "geom.bin", np.ones((12, 16, 20), np.uint8), 0.1, 0.1, 0.1)
+    write_optprops_file(tmp_path / "props.bid", [(0.3, 10.0, 0.9, 1.4)])
+    engine.write_safeprimes(tmp_path / "safeprimes_base32.txt", table[:230401])
+    (tmp_path / "p.txt").write_text("photons=5000\nseed=99\nabs_map=1\nsave_trans=1\n")
+    r = run(["geom.bin", "props.bid", "p.txt", "out"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    raw = (tmp_path / "out_abs.bin").read_bytes()
+    dims, nx, ny, nz = np.frombuffer(raw, "<i4", 4)
+    assert (dims, nx, ny, nz) == (3, 20, 16, 12)
+    A = np.frombuffer(raw, "<f8", offset=16 + 24)
+    F = np.frombuffer((tmp_path / "out_flu.bin").read_bytes(), "<f8", offset=40)
+    assert A.size == 20 * 16 * 12 and np.allclose(F, A / np.float32(0.3))
+    import json
+    rep = json.loads((tmp_path / "out_report.json").read_text())
+    assert abs(A.sum() - rep["absorbed"] / 2 ** 32 / 5000) < 1e-9
+    assert (tmp_path / "out_trans.bin").exists()

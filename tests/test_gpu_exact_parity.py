@@ -90,3 +90,19 @@ def test_batched_jobs(table):
     jobs = [m.Job(0, 0, 700, 11, "pencil"), m.Job(1, 1, 900, 22, "uniform"),
             m.Job(0, 0, 0, 33, "uniform"), m.Job(1, 1, 500, 44, "uniform", 7)]
     _compare([g1, g2], [p1, p2], jobs, table)
+
+
+def test_absorption_map(table):
+    """the per-voxel absorbed weight (the reference's disabled tally,
+    src/mc3d_gpu.cu:265-272) matches the oracle voxel for voxel and sums exactly to
+    the absorbed total; enabling it changes no other tally"""
+    g, p = layered(40, 36, 24, 0.1, air_holes=True)
+    job = m.Job(0, 0, 2500, 97531, "uniform")
+    r = m.run([g], [p], [job], table=table, math="exact", absorption_map=True)[0]
+    o = oracle_job(g, p, job, table, absorption_map=True)
+    assert np.array_equal(r.absorption, o["absorption"])
+    assert int(r.absorption.sum()) == r.totals["absorbed"]
+    plain = m.run([g], [p], [job], table=table, math="exact")[0]
+    assert plain.totals == r.totals and np.array_equal(plain.drs, r.drs)
+    fast = m.run([g], [p], [job], table=table, absorption_map=True)[0]
+    assert int(fast.absorption.sum()) == fast.totals["absorbed"]

@@ -65,7 +65,7 @@ class CTotals(C.Structure):
 
 class COut(C.Structure):
     _fields_ = [("drs", C.c_void_p), ("drs_sq", C.c_void_p), ("trans", C.c_void_p),
-                ("totals", CTotals)]
+                ("absorption", C.c_void_p), ("totals", CTotals)]
 
 
 PHOTON_RECORD_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("ux", "<f4"),
@@ -75,7 +75,8 @@ PHOTON_RECORD_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("ux",
 
 class COptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("math", C.c_int32), ("block", C.c_int32),
-                ("blocks_per_sm", C.c_int32), ("max_steps", C.c_int64),
+                ("blocks_per_sm", C.c_int32), ("absorption_map", C.c_int32),
+                ("reserved", C.c_int32), ("max_steps", C.c_int64),
                 ("photon_log", C.c_void_p), ("cancel", C.c_void_p)]
 
 
@@ -231,6 +232,7 @@ class Result:
     trans: np.ndarray     # uint64 [ny, nx]
     totals: dict
     photon_log: np.ndarray | None = None
+    absorption: np.ndarray | None = None  # uint64 [nz, ny, nx], sum Q(dW) per voxel
 
     @property
     def photons(self) -> int:
@@ -256,11 +258,12 @@ class Result:
 
 
 def _options(device=0, math="fast", block=0, blocks_per_sm=0, max_steps=0, log=None,
-             cancel=None) -> COptions:
+             cancel=None, absorption_map=False) -> COptions:
     o = COptions()
     lib().mc3d_default_options(C.byref(o))
     o.device, o.math, o.block, o.blocks_per_sm, o.max_steps = (
         device, MATH[math], block, blocks_per_sm, max_steps)
+    o.absorption_map = int(bool(absorption_map))
     o.photon_log = _ptr(log)
     o.cancel = _ptr(cancel)
     return o
@@ -273,16 +276,19 @@ def _arrays(geoms, props, jobs):
     return g, p, j
 
 
-def _outs(geoms, jobs):
+def _outs(geoms, jobs, absorption_map=False):
     res, outs = [], (COut * len(jobs))()
     for k, job in enumerate(jobs):
         if not 0 <= job.geom < len(geoms):
             raise Mc3dError(-1, f"job {k}: geometry index {job.geom} out of range")
-        nx, ny, _ = geoms[job.geom].shape
+        nx, ny, nz = geoms[job.geom].shape
         r = Result(np.zeros((ny, nx), np.uint64), np.zeros((ny, nx), np.uint64),
                    np.zeros((ny, nx), np.uint64), {})
         outs[k].drs, outs[k].drs_sq, outs[k].trans = (r.drs.ctypes.data, r.drs_sq.ctypes.data,
                                                       r.trans.ctypes.data)
+        if absorption_map:
+            r.absorption = np.zeros((nz, ny, nx), np.uint64)
+            outs[k].absorption = r.absorption.ctypes.data
         res.append(r)
     return res, outs
 
@@ -299,14 +305,16 @@ def _finish(res, outs, jobs, log):
 
 def run(geoms: Sequence[Geometry], props: Sequence[OpticalProps], jobs: Sequence[Job],
         table: np.ndarray | None = None, math: str = "fast", device: int = 0, block: int = 0,
-        blocks_per_sm: int = 0, max_steps: int = 0, photon_log: bool = False) -> list[Result]:
+        blocks_per_sm: int = 0, max_steps: int = 0, photon_log: bool = False,
+        absorption_map: bool = False) -> list[Result]:
     """Run every job in one persistent launch (mc3d_run)."""
     table = default_table() if table is None else np.ascontiguousarray(table, dtype=np.uint32)
     g, p, j = _arrays(geoms, props, jobs)
-    res, outs = _outs(geoms, jobs)
+    res, outs = _outs(geoms, jobs, absorption_map)
     log = (np.zeros(sum(int(x.photons) for x in jobs), PHOTON_RECORD_DTYPE)
            if photon_log else None)
-    opt = _options(device, math, block, blocks_per_sm, max_steps, log)
+    opt = _options(device, math, block, blocks_per_sm, max_steps, log,
+                   absorption_map=absorption_map)
     _check(lib().mc3d_run(g, len(geoms), p, len(props), j, len(jobs), table.ctypes.data,
                           len(table), C.byref(opt), outs))
     return _finish(res, outs, jobs, log)
@@ -327,6 +335,7 @@ class Plan:
                                       C.byref(opt)))
 
     def execute(self, stream: int | None = None) -> None:
+        """launch on `stream` (a cudaStream_t handle); None or 0 = the plan's own stream"""
         _check(lib().mc3d_plan_execute(self._h, stream))
 
     def read(self) -> list[Result]:

@@ -6,7 +6,7 @@
  * outname_simparam.dat.  The third argument, ignored by the reference
  * (README.md:38), is read as an optional key=value file:
  *   photons=30000000  seed=<time>  beam=uniform|pencil  streams=0  math=fast|exact
- *   safeprimes=safeprimes_base32.txt  max_steps=0  device=0
+ *   safeprimes=safeprimes_base32.txt  max_steps=0  device=0  abs_map=0  save_trans=0
  * An unreadable file (such as the README's "dummy_argument") keeps the defaults.
  * Differences: Total diffuse reflectance is the real total (the reference never
  * accumulates R_tot), and outname_report.json records the integer tallies.
@@ -36,6 +36,8 @@ struct Params {
     std::string safeprimes = "safeprimes_base32.txt";
     long long max_steps = 0;
     int device = 0;
+    bool abs_map = false;    /* write outname_abs.bin and outname_flu.bin */
+    bool save_trans = false; /* write outname_trans.bin */
 };
 
 std::string trim(const std::string &s)
@@ -63,6 +65,8 @@ bool read_params(const char *path, Params &p)
         else if (k == "safeprimes") p.safeprimes = v;
         else if (k == "max_steps") p.max_steps = std::stoll(v);
         else if (k == "device") p.device = std::stoi(v);
+        else if (k == "abs_map") p.abs_map = std::stoi(v) != 0;
+        else if (k == "save_trans") p.save_trans = std::stoi(v) != 0;
     }
     return true;
 }
@@ -139,12 +143,15 @@ int main(int argc, char *argv[])
     opt.device = prm.device;
     opt.math = prm.math;
     opt.max_steps = prm.max_steps;
+    opt.absorption_map = prm.abs_map ? 1 : 0;
 
     size_t nb = (size_t)nx * ny;
     std::vector<uint64_t> drs(nb), drs_sq(nb), trans(nb);
     mc3d_out out;
     memset(&out, 0, sizeof out);
     out.drs = drs.data(); out.drs_sq = drs_sq.data(); out.trans = trans.data();
+    std::vector<uint64_t> amap(prm.abs_map ? grid.size() : 0);
+    if (prm.abs_map) out.absorption = amap.data();
     auto t0 = std::chrono::steady_clock::now();
     st = mc3d_run(&geom, 1, &props, 1, &job, 1, table.data(), (int64_t)table.size(), &opt, &out);
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -173,6 +180,28 @@ int main(int argc, char *argv[])
     if (st) {
         fprintf(stderr, "The file was not saved.\n");
         return 1;
+    }
+    if (prm.save_trans) {
+        std::vector<double> Tn(nb);
+        for (size_t b = 0; b < nb; b++) Tn[b] = (double)trans[b] * q / finished;
+        mc3d_save_property((std::string(outName) + "_trans.bin").c_str(), 2, nx, ny, 1, (float)dx,
+                           (float)dy, 0.0, Tn.data());
+    }
+    if (prm.abs_map) {
+        /* save_abs_map (src/mc3d_io.cu:229-255, never called by the reference): absorbed
+         * weight per voxel per photon, and fluence = absorbed / mua of the voxel's
+         * tissue.  The reference multiplies by the photon count; dividing is what
+         * makes the map a fraction.  Voxels of mua = 0 get fluence 0, not inf. */
+        std::vector<double> A(grid.size()), F(grid.size());
+        for (size_t v = 0; v < grid.size(); v++) {
+            A[v] = (double)amap[v] * q / finished;
+            float m = mua[grid[v]];
+            F[v] = m > 0 ? A[v] / m : 0.0;
+        }
+        mc3d_save_property((std::string(outName) + "_abs.bin").c_str(), 3, nx, ny, nz, (float)dx,
+                           (float)dy, (float)dz, A.data());
+        mc3d_save_property((std::string(outName) + "_flu.bin").c_str(), 3, nx, ny, nz, (float)dx,
+                           (float)dy, (float)dz, F.data());
     }
     FILE *numPhotFile = fopen((std::string(outName) + "_simparam.dat").c_str(), "w");
     if (numPhotFile) {

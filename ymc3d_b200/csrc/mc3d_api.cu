@@ -134,6 +134,9 @@ struct mc3d_plan {
     uint32_t *d_mult = nullptr;
     RejectionDev *d_rej = nullptr;
     unsigned long long *d_tally = nullptr; /* drs | drs_sq | trans | totals | counter */
+    unsigned long long *d_amap = nullptr;  /* absorption map, all jobs' voxels */
+    std::vector<int64_t> job_voxels;
+    int64_t total_voxels = 0;
     PhotonRecord *d_log = nullptr;
     mc3d_photon_record *h_log = nullptr;
     volatile int32_t *h_cancel = nullptr;
@@ -156,6 +159,7 @@ static void plan_free(mc3d_plan *p)
     cudaFree(p->d_mult);
     cudaFree(p->d_rej);
     cudaFree(p->d_tally);
+    cudaFree(p->d_amap);
     cudaFree(p->d_log);
     if (p->cancel_registered) cudaHostUnregister((void *)p->h_cancel);
     if (p->stream) cudaStreamDestroy(p->stream);
@@ -238,7 +242,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     p->h_cancel = opt.cancel;
 
     std::vector<JobDev> jh(njobs);
-    int64_t stream_base = 0, bin_base = 0, photon_base = 0, scan_base = 0;
+    int64_t stream_base = 0, bin_base = 0, photon_base = 0, scan_base = 0, voxel_base = 0;
     for (int j = 0; j < njobs; j++) {
         const mc3d_job &jb = jobs[j];
         if (jb.geom < 0 || jb.geom >= ngeoms || jb.props < 0 || jb.props >= nprops) {
@@ -277,12 +281,16 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         d.remainder = jb.photons % S;
         d.bin_offset = bin_base;
         d.photon_base = photon_base;
+        d.amap_offset = voxel_base;
         d.seed = jb.seed;
         d.geom = jb.geom;
         d.props_offset = props_offset[jb.props];
         d.beam = jb.beam;
         int64_t bins = (int64_t)g.nx * g.ny;
+        int64_t voxels = bins * g.nz;
         p->job_bins.push_back(bins);
+        p->job_voxels.push_back(voxels);
+        voxel_base += voxels;
         p->job_photons.push_back(jb.photons);
         stream_base += count;
         d.stream_base_end = stream_base;
@@ -291,6 +299,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         photon_base += jb.photons;
     }
     p->total_bins = bin_base;
+    p->total_voxels = opt.absorption_map ? voxel_base : 0;
     p->total_photons = photon_base;
 
     int ndev = 0;
@@ -404,6 +413,8 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         PLAN_TRY(cudaMemcpyAsync(p->d_jobs, jh.data(), sizeof(JobDev) * njobs,
                                  cudaMemcpyHostToDevice, p->stream));
 
+    if (p->total_voxels)
+        PLAN_TRY(cudaMalloc(&p->d_amap, sizeof(unsigned long long) * p->total_voxels));
     if (p->h_log) PLAN_TRY(cudaMalloc(&p->d_log, sizeof(PhotonRecord) * std::max<int64_t>(1, p->total_photons)));
     if (p->h_cancel) {
         PLAN_TRY(cudaHostRegister((void *)p->h_cancel, sizeof(int32_t), cudaHostRegisterMapped));
@@ -444,6 +455,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     P.work_counter = p->d_tally + 3 * p->total_bins + (size_t)njobs * MC3D_NUM_TOTALS;
     P.cancel = p->d_cancel;
     P.photon_log = p->d_log;
+    P.amap = p->d_amap;
     P.num_multipliers = table_len;
     P.total_streams = stream_base;
     P.max_steps = opt.max_steps > 0 ? std::min<int64_t>(opt.max_steps, INT32_MAX) : (1 << 24);
@@ -463,6 +475,8 @@ int mc3d_plan_execute(mc3d_plan *p, void *stream)
     CUDA_TRY(cudaSetDevice(p->device));
     size_t tally_words = 3 * (size_t)p->total_bins + (size_t)p->njobs * MC3D_NUM_TOTALS + 1;
     CUDA_TRY(cudaMemsetAsync(p->d_tally, 0, tally_words * sizeof(unsigned long long), s));
+    if (p->d_amap)
+        CUDA_TRY(cudaMemsetAsync(p->d_amap, 0, sizeof(unsigned long long) * p->total_voxels, s));
     if (p->math == MC3D_MATH_FAST) CUDA_TRY(launch_photon_fast(p->P, p->grid, p->block, p->smem, s));
     else CUDA_TRY(launch_photon_exact(p->P, p->grid, p->block, p->smem, s));
     return MC3D_OK;
@@ -476,8 +490,14 @@ int mc3d_plan_read(mc3d_plan *p, mc3d_out *out)
     std::vector<unsigned long long> tot((size_t)p->njobs * MC3D_NUM_TOTALS);
     CUDA_TRY(cudaMemcpy(tot.data(), p->P.totals, tot.size() * sizeof(unsigned long long),
                         cudaMemcpyDeviceToHost));
-    int64_t off = 0;
+    int64_t off = 0, voff = 0;
     for (int j = 0; j < p->njobs; j++) {
+        if (out[j].absorption) {
+            if (!p->d_amap) return fail(MC3D_ERR_ARG, "absorption map not enabled in the plan");
+            CUDA_TRY(cudaMemcpy(out[j].absorption, p->d_amap + voff,
+                                sizeof(uint64_t) * p->job_voxels[j], cudaMemcpyDeviceToHost));
+        }
+        voff += p->job_voxels[j];
         size_t nb = (size_t)p->job_bins[j] * sizeof(uint64_t);
         if (out[j].drs) CUDA_TRY(cudaMemcpy(out[j].drs, p->P.drs + off, nb, cudaMemcpyDeviceToHost));
         if (out[j].drs_sq)

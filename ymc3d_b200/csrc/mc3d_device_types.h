@@ -36,6 +36,7 @@ struct JobDev {
     int64_t remainder;   /* photons mod S: streams below it run one extra photon */
     int64_t bin_offset;  /* first tally bin */
     int64_t photon_base; /* first record of the optional photon log */
+    int64_t amap_offset; /* first voxel of the job in the absorption map */
     uint64_t seed;       /* seeding-generator start (the reference's xinit) */
     int32_t geom;
     int32_t props_offset; /* first float4 of the job's optical table in shared memory */
@@ -70,6 +71,7 @@ struct KernelParams {
     unsigned long long *drs_sq; /* sum Q(W^2) */
     unsigned long long *trans;  /* sum Q(W) of photons frozen below the surface */
     unsigned long long *totals; /* njobs * MC3D_NUM_TOTALS */
+    unsigned long long *amap;   /* sum Q(dW) per voxel (absorption map variant only) */
     unsigned long long *work_counter;
     const int *cancel;
     PhotonRecord *photon_log;

@@ -170,11 +170,12 @@ struct Acc {
 
 /* One step of src/mc3d_gpu.cu:175-340 for a live photon.  Returns true when the
  * photon froze during this step; *db receives the step's boundary distance. */
-template <class M>
+template <class M, bool AMAP>
 static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float4 *tab,
                                                    Photon &p, uint64_t &rx, uint32_t ra,
                                                    const Acc &acc, float *db_out,
-                                                   uint32_t *fresnel_count)
+                                                   uint32_t *fresnel_count,
+                                                   unsigned long long *amap, bool *lat_mirror)
 {
     /* per tissue: (mua, mus, g, n), (mu_t, mua/mu_t, 1/mu_t, 1/(2g)),
      * (1-g^2, 1-g, 2g, 1+g^2) -- each the float the reference computes per step */
@@ -236,7 +237,17 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     /* absorption, src/mc3d_gpu.cu:262-263 */
     float W = p.W;
     float dW = (mu_t > 0) ? t1.y * W : 0;
+    float W_before = W;
     W = W - dW * (float)(!hit);
+    if (AMAP && !hit && mu_t > 0) {
+        /* absorption map, the reference's disabled tally (src/mc3d_gpu.cu:265-272):
+         * the current voxel clamped into the grid, fixed-point weight removed */
+        int ai = min(max(p.i, 0), g.nx - 1);
+        int aj = min(max(p.j, 0), g.ny - 1);
+        int ak = min(max(p.k, 0), g.nz - 1);
+        uint64_t dq = qw(W_before) - qw(W);
+        if (dq) atomicAdd(amap + ((int64_t)ak * g.ny + aj) * g.nx + ai, (unsigned long long)dq);
+    }
 
     /* russian roulette, src/mc3d_gpu.cu:275-277 */
     float eps = mc3d_rand_co(&rx, ra);
@@ -302,7 +313,9 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     p.z = !freeze ? newz : p.z;
 
     /* mirror boundary conditions, short-circuited as in src/mc3d_gpu.cu:330 */
+    bool fres_refl = refl;
     refl = refl || mirror(&p.x, &p.ux, g.Lx) || mirror(&p.y, &p.uy, g.Ly);
+    *lat_mirror = refl && !fres_refl;
 
     bool keep = (hit && refl) || freeze;
     p.i = keep ? p.i : nexti;
@@ -407,7 +420,7 @@ static __device__ __forceinline__ uint64_t stream_seed(const KernelParams &P, co
     return mc3d_seed_attempt(xs, P.seed.begin, fora);
 }
 
-template <class M>
+template <class M, bool AMAP>
 __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
 {
     extern __shared__ float4 sh_tab[];
@@ -429,6 +442,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
     uint32_t psteps = 0;
     uint32_t fresnel = 0;
     uint64_t qw0 = 0;
+    unsigned long long *amap = nullptr;
     const int64_t max_steps = P.max_steps;
 
     for (;;) {
@@ -442,6 +456,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
                 const JobDev &jb = P.jobs[job];
                 g = P.geoms[jb.geom];
                 tab = sh_tab + jb.props_offset;
+                if (AMAP) amap = P.amap + jb.amap_offset;
                 local = gs - jb.stream_base + jb.stream_first;
                 left = jb.per_stream + (local < jb.remainder ? 1 : 0);
                 ra = P.multipliers[1 + (local % (P.num_multipliers - 1))];
@@ -474,14 +489,20 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
         }
 
         float db;
-        bool froze = photon_step<M>(g, tab, p, rx, ra, acc, &db, &fresnel);
+        bool lat_mirror;
+        bool froze = photon_step<M, AMAP>(g, tab, p, rx, ra, acc, &db, &fresnel, amap,
+                                          &lat_mirror);
         chunk++;
         psteps++;
 
         bool done = false;
         uint64_t lost = 0;
         if (froze) {
-            db = masked_steps<M>(g, p, MC3D_NUM_PHOTON_STEPS - chunk, db);
+            /* If the freeze step's mirror did not fire and the photon is off the
+             * lateral faces, the masked steps change nothing and see the freeze
+             * step's boundary distance again: no need to replay them. */
+            if (lat_mirror || !(p.x > 0 && p.x < g.Lx && p.y > 0 && p.y < g.Ly))
+                db = masked_steps<M>(g, p, MC3D_NUM_PHOTON_STEPS - chunk, db);
             float w_before = p.W;
             if (quickfix(p, db)) { acc[T_QUICKFIX]++; lost = qw(w_before); }
             done = true;

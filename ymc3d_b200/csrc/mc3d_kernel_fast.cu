@@ -10,13 +10,21 @@ namespace mc3d {
 
 __global__ void __launch_bounds__(256, 3) photon_kernel_fast(const __grid_constant__ KernelParams P)
 {
-    photon_kernel_body<MathFast>(P);
+    photon_kernel_body<MathFast, false>(P);
+}
+
+/* with the per-voxel absorption map */
+__global__ void __launch_bounds__(256, 3)
+    photon_kernel_fast_amap(const __grid_constant__ KernelParams P)
+{
+    photon_kernel_body<MathFast, true>(P);
 }
 
 cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_t smem,
-                               cudaStream_t stream)
+                                cudaStream_t stream)
 {
-    photon_kernel_fast<<<grid, block, smem, stream>>>(P);
+    if (P.amap) photon_kernel_fast_amap<<<grid, block, smem, stream>>>(P);
+    else photon_kernel_fast<<<grid, block, smem, stream>>>(P);
     return cudaGetLastError();
 }
 
@@ -28,8 +36,11 @@ cudaError_t occupancy_photon_fast(int block, size_t smem, int *blocks_per_sm)
 
 cudaError_t smem_limit_photon_fast(size_t smem)
 {
-    return cudaFuncSetAttribute(photon_kernel_fast, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(photon_kernel_fast,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(photon_kernel_fast_amap,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 cudaError_t attributes_photon_fast(cudaFuncAttributes *attr)
