@@ -53,7 +53,10 @@ struct MathExact {
  * operators and functions below map to the approximate hardware paths. */
 struct MathFast {
     static constexpr bool kFast = true;
-    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
+    /* every denominator divided here is a direction cosine, a sum of products of
+     * cosines and sines, a refractive-index sum or 1 - g + 2 g xi, all far below the
+     * 2^126 where __fdividef stops being defined; x / 0 still gives +-inf or NaN */
+    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
     static __device__ __forceinline__ float div_r(float a, float, float r) { return a * r; }
     static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
     static __device__ __forceinline__ float rsqrt(float x) { return rsqrtf(x); }
@@ -312,9 +315,11 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     p.y = !freeze ? newy : p.y;
     p.z = !freeze ? newz : p.z;
 
-    /* mirror boundary conditions, short-circuited as in src/mc3d_gpu.cu:330 */
+    /* mirror boundary conditions, short-circuited as in src/mc3d_gpu.cu:330; off the
+     * lateral faces both mirrors are no-ops, which one rarely taken branch tests */
     bool fres_refl = refl;
-    refl = refl || mirror(&p.x, &p.ux, g.Lx) || mirror(&p.y, &p.uy, g.Ly);
+    if (!(p.x > 0 && p.x < g.Lx && p.y > 0 && p.y < g.Ly))
+        refl = refl || mirror(&p.x, &p.ux, g.Lx) || mirror(&p.y, &p.uy, g.Ly);
     *lat_mirror = refl && !fres_refl;
 
     bool keep = (hit && refl) || freeze;
