@@ -171,6 +171,32 @@ int mc3d_stream_seeds(const mc3d_job *job, const uint32_t *table, int64_t table_
 int mc3d_mwc_draws(const uint64_t *x, const uint32_t *a, int64_t ngen, int64_t n, float *out,
                    int32_t device);
 
+/* ------------------------------------------------- allocation-free entry point */
+
+/* No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc -- code inside a framework whose caching allocator owns the device
+ * memory (a raw cudaMalloc/cudaFree there synchronises the device and fragments
+ * the framework's pool), or a loop with a fixed memory budget.
+ *
+ * Runs one job (fast math) like mc3d_run, allocating nothing.  geom->tissue and
+ * the four outputs are DEVICE pointers the caller owns: drs, drs_sq and trans hold
+ * nx*ny words, totals the 14 words of mc3d_totals in its order; all four are
+ * overwritten.  props and table are host arrays.  The launch's working memory
+ * (descriptors, optical table, multipliers, rejection list, work counter) is one
+ * static device array of MC3D_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library holds until exit; inputs beyond its limits return MC3D_ERR_CAPACITY.
+ * All calls share that array: calls whose work overlaps on the GPU race, so run
+ * them one after another (the call returns once the kernel is queued on `stream`).
+ * The first call on a device looks up the array's address and should come before
+ * any stream capture. */
+#define MC3D_NOALLOC_SCRATCH_BYTES (1u << 20)
+#define MC3D_NOALLOC_MAX_TABLE 230401     /* safe-prime table lines */
+#define MC3D_NOALLOC_MAX_TISSUES 256
+#define MC3D_NOALLOC_MAX_REJECTIONS 4096  /* rejected seeding attempts in the job */
+int mc3d_run_noalloc(const mc3d_geom *geom, const mc3d_props *props, const mc3d_job *job,
+                     const uint32_t *table, int64_t table_len, int32_t device, void *stream,
+                     uint64_t *drs, uint64_t *drs_sq, uint64_t *trans, uint64_t *totals);
+
 /* ----------------------------------------------- reference-shaped entry point */
 
 /* Layout-compatible with geometry_t and opticalprops_t (src/mc3d_types.h:28-43). */

@@ -112,6 +112,9 @@ EXPORTS = {
                                     C.c_void_p, C.c_void_p, C.c_int32]),
     "mc3d_mwc_draws": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                  C.c_int32]),
+    "mc3d_run_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                   C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]),
     "mc3d_run_3dmc_gpu": (C.c_int, [CRefGeometry, CRefOptProps, C.c_int, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p]),

@@ -32,6 +32,7 @@ UNITS = {
                              "-Xptxas", "-v"],
     "mc3d_seed.cu": ["-fmad=false"],
     "mc3d_api.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"],
+    "mc3d_noalloc.cu": ["-use_fast_math", "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-v"],
 }
 CXX_UNITS = ["mc3d_safeprimes.cpp", "mc3d_io.cpp"]
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-pthread", "-ffp-contract=off", "-I", str(CSRC),

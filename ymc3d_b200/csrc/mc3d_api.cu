@@ -115,6 +115,20 @@ int list_rejections(const mc3d_seed_consts &sc, uint64_t seed, const uint32_t *t
 
 } /* namespace */
 
+/* the seeding helpers and the error text, for the other host files of the library */
+namespace mc3d {
+void set_last_error(const char *msg) { g_err = msg; }
+void make_seed_consts_host(uint32_t begin, mc3d_seed_consts *c) { make_seed_consts(begin, c); }
+int list_rejections_host(const mc3d_seed_consts &sc, uint64_t seed, const uint32_t *table,
+                         int64_t table_len, int64_t streams, int64_t first,
+                         std::vector<RejectionDev> &out, std::string *err)
+{
+    int st = list_rejections(sc, seed, table, table_len, streams, first, out);
+    if (st && err) *err = g_err;
+    return st;
+}
+} /* namespace mc3d */
+
 struct mc3d_plan {
     int device = 0;
     int math = MC3D_MATH_FAST;
