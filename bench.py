@@ -1,9 +1,7 @@
 """Benchmark: photons/s of the photon-tracking path on B200.
 
 Workload: the layered tissue with a vessel, 256x256x128 voxels of 0.02 mm, uniform
-beam, a job of 1e8 photons per GPU.  The job's RNG streams are split into --steps
-equal ranges and one step runs one range, so the K timed steps together are
-exactly the whole job (stream ranges of a job add up bit-for-bit to the job).
+beam, a job of 1e8 photons per GPU; one step is one launch of the whole job.
 
   value  device throughput: photons / kernel time, inputs resident in HBM, timed
          with CUDA events on the launching stream, L2 flushed between steps.
@@ -49,16 +47,25 @@ FP32_LANES_PER_SM, SFU_LANES_PER_SM = 128, 16
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--photons", type=float, default=1e8, help="photons per GPU per job")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--math", default="fast", choices=["fast", "exact"])
     ap.add_argument("--ref-photons", type=float, default=1e7)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--workload", default="layered",
+                    choices=["layered", "homogeneous", "sweep", "uneven", "deep"],
+                    help="layered is the headline; the others are the batched and "
+                         "special configurations, one launch per step")
+    ap.add_argument("--beam", default="uniform", choices=["uniform", "pencil"],
+                    help="beam of the sweep workload (the reference has only uniform)")
+    ap.add_argument("--photon-scale", type=float, default=0.01,
+                    help="photon budget factor of the sweep / uneven / deep workloads")
     return ap.parse_args()
 
 
@@ -175,16 +182,13 @@ def run_ours(args):
     w = layered_vessel(photons=per_gpu * world)
     job = w.jobs[0]
     S = job.num_streams()
-    K = max(1, args.steps)
 
-    def shard(k: int) -> "m.Job":
-        """stream range of step k (of K) owned by this rank"""
-        lo = (k % K) * S // K
-        hi = ((k % K) + 1) * S // K
-        first = lo + rank * (hi - lo) // world
-        last = lo + (rank + 1) * (hi - lo) // world
-        return m.Job(job.geom, job.props, job.photons, job.seed, job.beam, S,
-                     stream_first=first, stream_count=last - first)
+    def shard(j: "m.Job") -> "m.Job":
+        """this rank's stream range of job j"""
+        Sj = j.num_streams()
+        first = rank * Sj // world
+        return m.Job(j.geom, j.props, j.photons, j.seed, j.beam, Sj, stream_first=first,
+                     stream_count=(rank + 1) * Sj // world - first)
 
     g = w.geoms[0]
     pinned = torch.empty(g.tissue.size, dtype=torch.uint8, pin_memory=True)
@@ -194,9 +198,19 @@ def run_ours(args):
     pinned_tab = torch.empty(len(table), dtype=torch.int32, pin_memory=True)
     pinned_tab.numpy().view(np.uint32)[:] = table
     table_p = pinned_tab.numpy().view(np.uint32)
+    # warm-up job: the same workload at a tenth of the photons, another seed
+    warm_job = m.Job(job.geom, job.props, max(1, job.photons // 10), job.seed + 1, job.beam)
 
-    plans = [m.Plan([geom], w.props, [shard(k)], table=table_p, math=args.math, device=dev)
-             for k in range(K)]
+    tuned = {"block": 0, "blocks_per_sm": 0, "table": []}
+    if not args.no_tune:
+        from ymc3d_b200 import autotune
+        tuned = autotune.tune([geom], w.props, [shard(warm_job)], table=table_p, math=args.math,
+                              device=dev, use_cache=False)
+    shape = {"block": tuned["block"], "blocks_per_sm": tuned["blocks_per_sm"]}
+    plan = m.Plan([geom], w.props, [shard(job)], table=table_p, math=args.math, device=dev,
+                  **shape)
+    warm_plan = m.Plan([geom], w.props, [shard(warm_job)], table=table_p, math=args.math,
+                       device=dev, **shape)
     stream = torch.cuda.Stream(dev)  # a real stream handle (the legacy default stream is 0)
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
@@ -220,8 +234,8 @@ def run_ours(args):
         return res
 
     for k in range(args.warmup):
-        plans[k % K].execute(stream.cuda_stream)
-        exchange(plans[k % K].read())
+        warm_plan.execute(stream.cuda_stream)
+        exchange(warm_plan.read())
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
@@ -233,12 +247,12 @@ def run_ours(args):
             torch.cuda.synchronize(dev)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            plans[k].execute(stream.cuda_stream)
+            plan.execute(stream.cuda_stream)
             e1.record(stream)
             e1.synchronize()
             launches += 1
             times.append(e0.elapsed_time(e1) / 1e3)
-            res = exchange(plans[k].read())
+            res = exchange(plan.read())
             steps_tot += res[0].totals["steps"]
             fresnel_tot += res[0].totals["fresnel"]
             photons_tot += res[0].totals["photons"]
@@ -257,13 +271,14 @@ def run_ours(args):
         h2d = g.tissue.size + table_p.nbytes + sum(p.mua.nbytes * 4 for p in w.props)
         d2h = 3 * nb * 8 + 14 * 8
         e2e_photons = 0
-        for k in range(max(1, min(args.e2e_steps, K))):
+        for k in range(max(1, args.e2e_steps)):
             flush.fill_(k & 0xff)
             torch.cuda.synchronize(dev)
             if dist:
                 dist.barrier()
             t0 = time.perf_counter()
-            res = m.run([geom], w.props, [shard(k)], table=table_p, math=args.math, device=dev)
+            res = m.run([geom], w.props, [shard(job)], table=table_p, math=args.math, device=dev,
+                        **shape)
             res = exchange(res)
             e2e_times.append(time.perf_counter() - t0)
             e2e_photons += res[0].totals["photons"]
@@ -278,8 +293,8 @@ def run_ours(args):
                          "kernel, read-back), max over ranks"}
 
     if rank != 0:
-        for pl in plans:
-            pl.close()
+        plan.close()
+        warm_plan.close()
         if dist:
             dist.barrier()
             dist.destroy_process_group()
@@ -301,7 +316,7 @@ def run_ours(args):
             traffic = json.loads(tp.read_text()).get("bytes_per_launch")
         except Exception:
             traffic = None
-    block, grid, smem = plans[0].shape()
+    block, grid, smem = plan.shape()
     line = {
         "metric": "photons/s (layered tissue + vessel, 256x256x128, uniform beam, 1 B200)",
         "value": value, "unit": "photons/s", "n_gpus": world, "steps": args.steps,
@@ -310,10 +325,12 @@ def run_ours(args):
         "data": "synthetic (seeded layered-tissue geometry, reference input formats)",
         "config": {"workload": w.name, "photons_per_job": int(job.photons),
                    "photons_per_step": int(photons_step),
-                   "step": f"1/{K} of the job's RNG streams; the {K} timed steps are the "
-                           "whole job", "voxels": list(g.shape), "voxel_mm": g.dx,
+                   "step": "one launch of the whole job (each rank: its stream shard)",
+                   "warmup": "3 launches of the same workload at a tenth of the photons", "voxels": list(g.shape), "voxel_mm": g.dx,
                    "beam": "uniform", "math": args.math, "streams": S,
-                   "launch": {"block": block, "grid": grid, "smem": smem},
+                   "launch": {"block": block, "grid": grid, "smem": smem,
+                              "autotuner": [{k: r[k] for k in ("block", "blocks_per_sm", "ms")}
+                                            for r in tuned["table"]]},
                    "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"{world} ranks, disjoint stream shards, NCCL sum of tallies"},
         "steps_per_s": steps_per_s * world,
@@ -331,12 +348,43 @@ def run_ours(args):
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
-    for pl in plans:
-        pl.close()
+    plan.close()
+    warm_plan.close()
     print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_reference_sweep(args, exe: Path):
+    """The reference binary once per wavelength of the sweep (uniform beam: its
+    pencil branch is compiled out), timed as the sum of its run_3dmc_gpu calls."""
+    from ymc3d_b200.workloads import sweep, write_geometry_file, write_optprops_file
+    w = sweep(photon_scale=args.photon_scale, beam="uniform")
+    g = w.geoms[0]
+    tmp = Path(tempfile.mkdtemp())
+    write_geometry_file(tmp / "geom.bin", g.tissue, g.dx, g.dy, g.dz)
+    secs, fins = 0.0, 0
+    for k, job in enumerate(w.jobs):
+        p = w.props[job.props]
+        rows = np.stack([p.mua, p.mus, p.g, p.n], 1)[1:]
+        write_optprops_file(tmp / f"p{k}.bid", rows)
+        subprocess.run([str(exe), str(tmp / "geom.bin"), str(tmp / f"p{k}.bid"),
+                        str(int(job.photons)), str(int(job.seed) & 0xffffffff or 1),
+                        str(tmp / f"r{k}"), str(exe.parent)], check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        raw = (tmp / f"r{k}_ref.bin").read_bytes()
+        fins += int(np.frombuffer(raw, "<i8", 1)[0])
+        secs += float(np.frombuffer(raw, "<f8", 1, offset=8)[0])
+    line = {"metric": f"photons/s ({w.name}, uniform beam, 1 B200)", "value": fins / secs,
+            "unit": "photons/s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": w.name, "jobs": len(w.jobs), "photons_per_step": fins,
+                       "photon_scale": args.photon_scale,
+                       "how": "one run_3dmc_gpu call per wavelength, summed"},
+            "impl": "reference"}
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(args):
@@ -344,6 +392,13 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if args.workload == "sweep":
+        exe = ROOT / "oracle" / "_ref" / "gpu-mc-ref"
+        if not exe.exists():
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "oracle/_ref/gpu-mc-ref not built (oracle/build_ref.py)"}))
+            return
+        return run_reference_sweep(args, exe)
     exe = ROOT / "oracle" / "_ref" / "gpu-mc-ref"
     if not exe.exists():
         print(json.dumps({"impl": "reference", "unavailable":
@@ -392,10 +447,83 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args):
+    """One persistent launch over every job of a batched workload, timed like the
+    headline (CUDA events on the launching stream, L2 flushed between steps),
+    beside the same jobs launched one by one ("plain")."""
+    import torch
+
+    import ymc3d_b200 as m
+    from ymc3d_b200 import workloads as W
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(dev)
+    if args.workload == "homogeneous":
+        w = W.homogeneous(photons=int(1e6))
+    elif args.workload == "sweep":
+        w = W.sweep(photon_scale=args.photon_scale, beam=args.beam)
+    elif args.workload == "uneven":
+        w = W.uneven(photons=max(1, int(1e7 * args.photon_scale)))
+    else:
+        w = W.deep_grid(photons=max(1, int(1e9 * args.photon_scale)))
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def timed(plan, steps, warmup):
+        for _ in range(warmup):
+            plan.execute(stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        ts, res = [], None
+        for k in range(steps):
+            flush.fill_(k & 0xff)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.execute(stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+            res = plan.read()
+        return sum(ts) / len(ts), res
+
+    with ClockSampler(dev) as clocks:
+        plan = m.Plan(w.geoms, w.props, w.jobs, math=args.math, device=dev)
+        t_batch, res = timed(plan, args.steps, args.warmup)
+        plan.close()
+        photons = sum(r.photons for r in res)
+        steps = sum(r.totals["steps"] for r in res)
+        plain = None
+        if len(w.jobs) > 1:
+            t_plain = 0.0
+            for job in w.jobs:
+                pl = m.Plan([w.geoms[job.geom]], [w.props[job.props]],
+                            [m.Job(0, 0, job.photons, job.seed, job.beam)], math=args.math,
+                            device=dev)
+                t, _ = timed(pl, 1, 1)
+                t_plain += t
+                pl.close()
+            plain = {"value": photons / t_plain, "unit": "photons/s",
+                     "ms_per_batch": t_plain * 1e3,
+                     "how": f"{len(w.jobs)} launches, one job each, same seeds"}
+    line = {"metric": f"photons/s ({w.name}, 1 B200)", "value": photons / t_batch,
+            "unit": "photons/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_batch * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+u64", "data": "synthetic (seeded)",
+            "config": {"workload": w.name, "jobs": len(w.jobs), "photons_per_step": photons,
+                       "math": args.math, "photon_scale": args.photon_scale},
+            "steps_per_s": steps / t_batch, "plain": plain, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "layered":
+        run_batched(args)
     else:
         run_ours(args)
 

@@ -73,14 +73,15 @@ typedef struct {
     int32_t beam;     /* enum mc3d_beam */
     int32_t pad;
     int64_t photons;
-    int64_t streams;  /* 0: min(photons, MC3D_DEFAULT_STREAMS) */
+    int64_t streams;  /* 0: min(photons, MC3D_DEFAULT_STREAMS), i.e. one photon per stream,
+                         which balances a launch at photon granularity */
     uint64_t seed;    /* the reference's xinit; must satisfy init_RNG's check */
     int64_t stream_first; /* run only streams [stream_first, stream_first + stream_count): */
     int64_t stream_count; /* one shard of the job; 0 = all streams.  Shards' tallies add up
                              exactly to the whole job's */
 } mc3d_job;
 
-#define MC3D_DEFAULT_STREAMS 4194304
+#define MC3D_DEFAULT_STREAMS (1ll << 40) /* the jump-ahead covers 2^40 seeding attempts */
 
 /* Per-job totals.  Conservation, exact in integers:
  *   w_launched = r_in + r_out + t_in + t_out + absorbed + rr_killed - rr_created + lost */
@@ -127,7 +128,8 @@ typedef struct {
     int32_t block;          /* threads per block, 0 = tuned */
     int32_t blocks_per_sm;  /* 0 = as many as fit */
     int32_t absorption_map; /* 1: tally absorbed weight per voxel (sum over voxels = absorbed) */
-    int32_t reserved;
+    int32_t use_graph;      /* 1: a plan's first execute captures the tally clear and the
+                               launch into a CUDA graph, later executes replay it */
     int64_t max_steps;      /* per-photon step cap, 0 = 2^24 */
     mc3d_photon_record *photon_log; /* host, sum of photons over jobs, or NULL */
     volatile int32_t *cancel;       /* optional host flag, read when a stream starts */

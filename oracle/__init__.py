@@ -13,6 +13,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "liboracle.so"
+LIB64_PATH = HERE / "liboracle64.so"  # the same loop in FP64 with libm functions
 TOTAL_FIELDS = ("photons", "steps", "w_launched", "r_in", "r_out", "t_in", "t_out", "absorbed",
                 "rr_killed", "rr_created", "lost", "capped", "quickfix", "fresnel")
 REC_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("ux", "<f4"), ("uy", "<f4"),
@@ -37,15 +38,17 @@ class OJob(C.Structure):
 
 
 _lib = None
+_lib64 = None
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not LIB_PATH.exists():
+def lib(f64: bool = False):
+    global _lib, _lib64
+    if (_lib64 if f64 else _lib) is None:
+        path = LIB64_PATH if f64 else LIB_PATH
+        if not path.exists():
             from . import build as _b
             _b.build()
-        h = C.CDLL(str(LIB_PATH))
+        h = C.CDLL(str(path))
         h.orc_init_rng.restype = C.c_int
         h.orc_init_rng.argtypes = [C.c_void_p, C.c_int64, C.c_uint64, C.c_int64, C.c_void_p,
                                    C.c_void_p]
@@ -62,8 +65,11 @@ def lib():
         h.orc_sincospif.argtypes = [C.c_float, C.c_void_p, C.c_void_p]
         h.orc_grid_coord_x.restype = C.c_int
         h.orc_grid_coord_x.argtypes = [C.c_float, C.c_float, C.c_float]
-        _lib = h
-    return _lib
+        if f64:
+            _lib64 = h
+        else:
+            _lib = h
+    return _lib64 if f64 else _lib
 
 
 def init_rng(table: np.ndarray, seed: int, n: int):
@@ -87,9 +93,10 @@ def rand_co(x: int, a: int, n: int) -> np.ndarray:
 def run(tissue: np.ndarray, dx: float, dy: float, dz: float, mua, mus, g, n, photons: int,
         streams: int, seed: int, table: np.ndarray, beam: int = 0, threads: int = 0,
         first: int = 0, count: int = -1, max_steps: int = 0, photon_log: bool = False,
-        absorption_map: bool = False):
+        absorption_map: bool = False, f64: bool = False):
     """Simulate streams [first, first+count) of a job; returns dict with drs, drs_sq,
-    trans ([ny, nx] uint64), totals and the optional per-photon log."""
+    trans ([ny, nx] uint64), totals and the optional per-photon log.  f64 runs the
+    FP64 build of the same loop (geometry in the file's double voxel sizes)."""
     tissue = np.ascontiguousarray(tissue, np.uint8)
     nz, ny, nx = tissue.shape
     arrs = [np.ascontiguousarray(v, np.float32) for v in (mua, mus, g, n)]
@@ -103,7 +110,7 @@ def run(tissue: np.ndarray, dx: float, dy: float, dz: float, mua, mus, g, n, pho
     tot = np.zeros(len(TOTAL_FIELDS), np.uint64)
     log = np.zeros(max(photons, 1), REC_DTYPE) if photon_log else None
     amap = np.zeros((nz, ny, nx), np.uint64) if absorption_map else None
-    st = lib().orc_run(C.byref(geom), C.byref(props), C.byref(job), table.ctypes.data,
+    st = lib(f64).orc_run(C.byref(geom), C.byref(props), C.byref(job), table.ctypes.data,
                        len(table), threads, first, count, drs.ctypes.data, drs_sq.ctypes.data,
                        trans.ctypes.data, tot.ctypes.data,
                        None if log is None else log.ctypes.data,

@@ -35,6 +35,37 @@
 
 #include "../ymc3d_b200/csrc/mc3d_exactmath.h"
 
+/* The transport arithmetic type.  The default build is FP32, like the reference,
+ * with the reproducible series functions; -DORC_F64 builds the same loop in FP64
+ * with libm's functions, the precision reference for FP32 results. */
+#ifdef ORC_F64
+typedef double real;
+#define R_FMIN fmin
+#define R_FLOOR floor
+#define R_FABS fabs
+#define R_COPYSIGN copysign
+#define R_SQRT sqrt
+#define R_LOG log
+#define R_ACOS acos
+#define R_SIN sin
+static void r_sincospi(double x, double *s, double *c)
+{
+    *s = sin(3.14159265358979323846 * x);
+    *c = cos(3.14159265358979323846 * x);
+}
+#else
+typedef float real;
+#define R_FMIN fminf
+#define R_FLOOR floorf
+#define R_FABS fabsf
+#define R_COPYSIGN copysignf
+#define R_SQRT sqrtf
+#define R_LOG mc3d_xm_logf
+#define R_ACOS mc3d_xm_acosf
+#define R_SIN mc3d_xm_sinf
+#define r_sincospi mc3d_xm_sincospif
+#endif
+
 #define ORC_SURVIVAL_CHANCE 0.1 /* src/mc3d_types.h:11-18 */
 #define ORC_W_THRESHOLD 0.0001
 #define ORC_UZ_THRESH 0.99999
@@ -119,35 +150,35 @@ int orc_init_rng(const uint32_t *table, int64_t table_len, uint64_t xinit, int64
 
 /* --------------------------------------------------------------- helpers */
 
-/* float -> int as the GPU converts (saturating, NaN -> 0) */
-static int orc_f2i(float v)
+/* real -> int as the GPU converts (saturating, NaN -> 0) */
+static int orc_f2i(real v)
 {
     if (v != v) return 0;
-    if (v >= 2147483648.0f) return INT32_MAX;
-    if (v < -2147483648.0f) return INT32_MIN;
+    if (v >= (real)2147483648.0) return INT32_MAX;
+    if (v < (real)-2147483648.0) return INT32_MIN;
     return (int)v;
 }
 
 static int orc_inc(int i) { return (int)((unsigned)i + 1u); }
 
-static int orc_grid_coord(float x, float ux, float d)
+static int orc_grid_coord(real x, real ux, real d)
 {
-    int i = orc_f2i(floorf(x / d));
-    i += (x == (float)orc_inc(i) * d);
-    float bmin = (float)i * d;
+    int i = orc_f2i(R_FLOOR(x / d));
+    i += (x == (real)orc_inc(i) * d);
+    real bmin = (real)i * d;
     i = ((x > bmin) || ((x == bmin) && (ux >= 0))) ? i : i - 1;
     return i;
 }
 
 typedef struct {
     int nx, ny, nz;
-    float dx, dy, dz, Lx, Ly, Lz;
+    real dx, dy, dz, Lx, Ly, Lz;
     const uint8_t *tissue;
 } orc_g;
 
 static int orc_clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-static int orc_tissue(const orc_g *g, int i, int j, int k, float z, float uz)
+static int orc_tissue(const orc_g *g, int i, int j, int k, real z, real uz)
 {
     int ci = orc_clampi(i, 0, g->nx - 1);
     int cj = orc_clampi(j, 0, g->ny - 1);
@@ -156,71 +187,71 @@ static int orc_tissue(const orc_g *g, int i, int j, int k, float z, float uz)
     return ((z <= 0) && (uz < 0)) ? ORC_AIR : t;
 }
 
-static float orc_intersection(const orc_g *g, int i, int j, int k, float *x, float ux, float *y,
-                              float uy, float *z, float uz)
+static real orc_intersection(const orc_g *g, int i, int j, int k, real *x, real ux, real *y,
+                              real uy, real *z, real uz)
 {
-    float border_x = (float)((ux >= 0) ? orc_inc(i) : i) * g->dx;
-    float t_x = (border_x - *x) / ux;
-    float border_y = (float)((uy >= 0) ? orc_inc(j) : j) * g->dy;
-    float t_y = (border_y - *y) / uy;
-    float border_z = (float)((uz >= 0) ? orc_inc(k) : k) * g->dz;
-    float t_z = (border_z - *z) / uz;
-    float t = fminf(t_x, fminf(t_y, t_z));
+    real border_x = (real)((ux >= 0) ? orc_inc(i) : i) * g->dx;
+    real t_x = (border_x - *x) / ux;
+    real border_y = (real)((uy >= 0) ? orc_inc(j) : j) * g->dy;
+    real t_y = (border_y - *y) / uy;
+    real border_z = (real)((uz >= 0) ? orc_inc(k) : k) * g->dz;
+    real t_z = (border_z - *z) / uz;
+    real t = R_FMIN(t_x, R_FMIN(t_y, t_z));
     *x = (t == t_x) ? border_x : *x + ux * t;
     *y = (t == t_y) ? border_y : *y + uy * t;
     *z = (t == t_z) ? border_z : *z + uz * t;
     return t;
 }
 
-static int orc_mirror(float *x, float *ux, float length)
+static int orc_mirror(real *x, real *ux, real length)
 {
     int refl = (*x >= length) || (*x <= 0);
     *x = (*x >= length) ? 2 * length - *x : *x;
-    *x = (*x <= 0) ? fabsf(*x) : *x;
+    *x = (*x <= 0) ? R_FABS(*x) : *x;
     *ux = refl ? -1 * (*ux) : *ux;
     return refl;
 }
 
-static uint64_t orc_q(float w)
+static uint64_t orc_q(real w)
 {
-    double v = nearbyint((double)(w * 4294967296.0f));
+    double v = nearbyint((double)(w * (real)4294967296.0));
     if (!(v > 0)) return 0; /* negative and NaN convert to 0, as cvt.rni.u64 does */
     if (v >= 18446744073709551616.0) return UINT64_MAX;
     return (uint64_t)v;
 }
 
 typedef struct {
-    float x, y, z, ux, uy, uz, W, s;
+    real x, y, z, ux, uy, uz, W, s;
     int i, j, k, tissue;
 } orc_ph;
 
 typedef struct {
-    const float *mua, *mus, *g, *n;
+    const real *mua, *mus, *g, *n;
 } orc_tab;
 
 /* photontrack_step body for one live photon; returns 1 on freeze */
 static int orc_step(const orc_g *G, const orc_tab *P, orc_ph *p, uint64_t *rx, uint32_t ra,
-                    uint64_t *killed, uint64_t *created, float *db_out, uint64_t *fresnel,
+                    uint64_t *killed, uint64_t *created, real *db_out, uint64_t *fresnel,
                     uint64_t *amap)
 {
     int tissue_type = p->tissue;
-    float ni = P->n[tissue_type];
-    float nt = ni;
-    float epsilon;
-    float mu_a = P->mua[tissue_type];
-    float mu_s = P->mus[tissue_type];
-    float g = P->g[tissue_type];
-    float mu_t = mu_a + mu_s;
+    real ni = P->n[tissue_type];
+    real nt = ni;
+    real epsilon;
+    real mu_a = P->mua[tissue_type];
+    real mu_s = P->mus[tissue_type];
+    real g = P->g[tissue_type];
+    real mu_t = mu_a + mu_s;
 
-    float newx = p->x, newy = p->y, newz = p->z;
-    float db = orc_intersection(G, p->i, p->j, p->k, &newx, p->ux, &newy, p->uy, &newz, p->uz);
+    real newx = p->x, newy = p->y, newz = p->z;
+    real db = orc_intersection(G, p->i, p->j, p->k, &newx, p->ux, &newy, p->uy, &newz, p->uz);
 
     int hit_boundary = db * mu_t <= p->s;
-    float ds = hit_boundary ? db * mu_t : p->s;
+    real ds = hit_boundary ? db * mu_t : p->s;
     newx = hit_boundary ? newx : p->x + p->ux * ds / mu_t;
     newy = hit_boundary ? newy : p->y + p->uy * ds / mu_t;
     newz = hit_boundary ? newz : p->z + p->uz * ds / mu_t;
-    float s = p->s - ds;
+    real s = p->s - ds;
 
     int nexti = orc_grid_coord(newx, p->ux, G->dx);
     int nextj = orc_grid_coord(newy, p->uy, G->dy);
@@ -228,41 +259,41 @@ static int orc_step(const orc_g *G, const orc_tab *P, orc_ph *p, uint64_t *rx, u
     int next_tissue_type = orc_tissue(G, nexti, nextj, nextk, newz, p->uz);
     nt = P->n[next_tissue_type];
 
-    float ux = p->ux, uy = p->uy, uz = p->uz;
-    float transrefl_ux = ux, transrefl_uy = uy, transrefl_uz = uz;
+    real ux = p->ux, uy = p->uy, uz = p->uz;
+    real transrefl_ux = ux, transrefl_uy = uy, transrefl_uz = uz;
     int isReflected = 0;
     if (ni != nt) {
-        float cos_ai = (p->i != nexti) ? ux : ((p->j != nextj) ? uy : uz);
-        cos_ai = fabsf(cos_ai);
+        real cos_ai = (p->i != nexti) ? ux : ((p->j != nextj) ? uy : uz);
+        cos_ai = R_FABS(cos_ai);
         cos_ai = (cos_ai > 1) ? 1 : cos_ai;
-        float ai = mc3d_xm_acosf(cos_ai);
-        float ni_nt = ni / nt;
-        float sin_ai = mc3d_xm_sinf(ai);
-        float sin_at = ni_nt * sin_ai;
-        float cos_at = sqrtf(1.0f - sin_at * sin_at);
-        float R1 = (sin_ai * cos_at - cos_ai * sin_at) / (sin_ai * cos_at + cos_ai * sin_at);
-        float R2 = (cos_ai * cos_at - sin_ai * sin_at) / (cos_ai * cos_at + sin_at * sin_at);
-        float R = 0.5 * R1 * R1 * (1.0f + R2 * R2);
+        real ai = R_ACOS(cos_ai);
+        real ni_nt = ni / nt;
+        real sin_ai = R_SIN(ai);
+        real sin_at = ni_nt * sin_ai;
+        real cos_at = R_SQRT((real)1 - sin_at * sin_at);
+        real R1 = (sin_ai * cos_at - cos_ai * sin_at) / (sin_ai * cos_at + cos_ai * sin_at);
+        real R2 = (cos_ai * cos_at - sin_ai * sin_at) / (cos_ai * cos_at + sin_at * sin_at);
+        real R = 0.5 * R1 * R1 * ((real)1 + R2 * R2);
         R = (sin_at > 1) ? 1 : R;
         R = (ni == nt) ? 0 : R;
         epsilon = orc_rand_co1(rx, ra);
         isReflected = epsilon < R;
         transrefl_ux = isReflected ? ux * ((p->i == nexti) ? 1 : -1)
-                                   : ((p->i != nexti) ? copysignf(cos_at, ux * cos_at) : ux * ni_nt);
+                                   : ((p->i != nexti) ? R_COPYSIGN(cos_at, ux * cos_at) : ux * ni_nt);
         transrefl_uy = isReflected ? uy * ((p->j == nextj) ? 1 : -1)
                                    : (((p->j != nextj) && (p->i == nexti))
-                                          ? copysignf(cos_at, uy * cos_at)
+                                          ? R_COPYSIGN(cos_at, uy * cos_at)
                                           : uy * ni_nt);
         transrefl_uz = isReflected ? uz * ((p->k == nextk) ? 1 : -1)
                                    : (((p->k != nextk) && (p->j == nextj) && (p->i == nexti))
-                                          ? copysignf(cos_at, uz * cos_at)
+                                          ? R_COPYSIGN(cos_at, uz * cos_at)
                                           : uz * ni_nt);
         (*fresnel)++;
     }
 
-    float W = p->W;
-    float dW = (mu_t > 0) ? mu_a / mu_t * W : 0;
-    W = W - dW * (float)(!hit_boundary);
+    real W = p->W;
+    real dW = (mu_t > 0) ? mu_a / mu_t * W : 0;
+    W = W - dW * (real)(!hit_boundary);
     if (amap && (!hit_boundary) && (mu_t > 0)) {
         /* the reference's disabled absorption tally (src/mc3d_gpu.cu:265-272) */
         int abs_i = orc_clampi(p->i, 0, G->nx - 1);
@@ -274,38 +305,38 @@ static int orc_step(const orc_g *G, const orc_tab *P, orc_ph *p, uint64_t *rx, u
     }
 
     epsilon = orc_rand_co1(rx, ra);
-    float newW = (epsilon < ORC_SURVIVAL_CHANCE) ? (float)(W / ORC_SURVIVAL_CHANCE) : 0;
+    real newW = (epsilon < ORC_SURVIVAL_CHANCE) ? (real)(W / ORC_SURVIVAL_CHANCE) : 0;
     if ((W < ORC_W_THRESHOLD) && (!hit_boundary) && (mu_t != 0)) {
         if (newW == 0.0f) *killed += orc_q(W);
         else *created += orc_q(newW) - orc_q(W);
         W = newW;
     }
 
-    float costheta = (1 - g * g) / (1 - g + 2 * g * orc_rand_oc1(rx, ra));
-    costheta = 1.0f / (2 * g) * (1 + g * g - costheta * costheta);
-    float sintheta = sqrtf(1 - costheta * costheta);
-    float phi_divpi = 2 * orc_rand_co1(rx, ra);
-    float cosphi, sinphi;
-    mc3d_xm_sincospif(phi_divpi, &sinphi, &cosphi);
-    float invsqrt = 1.0f / sqrtf(1 - uz * uz);
-    float scatt_ux = (fabsf(uz) <= ORC_UZ_THRESH)
+    real costheta = (1 - g * g) / (1 - g + 2 * g * orc_rand_oc1(rx, ra));
+    costheta = (real)1 / (2 * g) * (1 + g * g - costheta * costheta);
+    real sintheta = R_SQRT(1 - costheta * costheta);
+    real phi_divpi = 2 * orc_rand_co1(rx, ra);
+    real cosphi, sinphi;
+    r_sincospi(phi_divpi, &sinphi, &cosphi);
+    real invsqrt = (real)1 / R_SQRT(1 - uz * uz);
+    real scatt_ux = (R_FABS(uz) <= ORC_UZ_THRESH)
                          ? sintheta * (ux * uz * cosphi - uy * sinphi) * invsqrt + ux * costheta
                          : sintheta * cosphi;
-    float scatt_uy = (fabsf(uz) <= ORC_UZ_THRESH)
+    real scatt_uy = (R_FABS(uz) <= ORC_UZ_THRESH)
                          ? sintheta * (uy * uz * cosphi + ux * sinphi) * invsqrt + uy * costheta
                          : sintheta * sinphi;
-    float scatt_uz = (fabsf(uz) <= ORC_UZ_THRESH)
-                         ? -1 * sqrtf(1 - uz * uz) * sintheta * cosphi + uz * costheta
-                         : copysignf(costheta, costheta * uz);
+    real scatt_uz = (R_FABS(uz) <= ORC_UZ_THRESH)
+                         ? -1 * R_SQRT(1 - uz * uz) * sintheta * cosphi + uz * costheta
+                         : R_COPYSIGN(costheta, costheta * uz);
 
-    float newux = (!hit_boundary) ? scatt_ux : transrefl_ux;
-    float newuy = (!hit_boundary) ? scatt_uy : transrefl_uy;
-    float newuz = (!hit_boundary) ? scatt_uz : transrefl_uz;
-    float zero_thresh = 1 - ORC_UZ_THRESH;
-    newux = (fabsf(newux) < zero_thresh) ? 0 : newux;
-    newuy = (fabsf(newuy) < zero_thresh) ? 0 : newuy;
-    newuz = (fabsf(newuz) < zero_thresh) ? 0 : newuz;
-    float newu_norm = 1.0f / sqrtf(newux * newux + newuy * newuy + newuz * newuz);
+    real newux = (!hit_boundary) ? scatt_ux : transrefl_ux;
+    real newuy = (!hit_boundary) ? scatt_uy : transrefl_uy;
+    real newuz = (!hit_boundary) ? scatt_uz : transrefl_uz;
+    real zero_thresh = 1 - ORC_UZ_THRESH;
+    newux = (R_FABS(newux) < zero_thresh) ? 0 : newux;
+    newuy = (R_FABS(newuy) < zero_thresh) ? 0 : newuy;
+    newuz = (R_FABS(newuz) < zero_thresh) ? 0 : newuz;
+    real newu_norm = (real)1 / R_SQRT(newux * newux + newuy * newuy + newuz * newuz);
     newux *= newu_norm;
     newuy *= newu_norm;
     newuz *= newu_norm;
@@ -316,7 +347,7 @@ static int orc_step(const orc_g *G, const orc_tab *P, orc_ph *p, uint64_t *rx, u
     p->uz = (!freeze) ? newuz : uz;
 
     epsilon = orc_rand_oc1(rx, ra);
-    float newS = (W > 0) ? -mc3d_xm_logf(epsilon) : 0;
+    real newS = (W > 0) ? -R_LOG(epsilon) : 0;
     p->s = (freeze || hit_boundary) ? s : newS;
     p->W = W;
 
@@ -343,7 +374,7 @@ static void orc_derive(const orc_g *G, orc_ph *p)
     p->tissue = orc_tissue(G, p->i, p->j, p->k, p->z, p->uz);
 }
 
-static int orc_quickfix(orc_ph *p, float db)
+static int orc_quickfix(orc_ph *p, real db)
 {
     if (isinf(p->x) || isnan(p->x) || isinf(p->y) || isnan(p->y) || isinf(p->z) || isnan(p->z) ||
         isinf(p->s) || isnan(p->s) || isinf(p->ux) || isnan(p->ux) || isinf(p->uy) ||
@@ -375,11 +406,11 @@ static void orc_photon(const orc_g *G, const orc_tab *P, int beam, int64_t max_s
     }
     p.z = 0;
     p.ux = 0; p.uy = 0; p.uz = 1;
-    float n0 = P->n[ORC_AIR], n1 = P->n[1];
-    float Rsp = (n0 - n1) / (n0 + n1);
+    real n0 = P->n[ORC_AIR], n1 = P->n[1];
+    real Rsp = (n0 - n1) / (n0 + n1);
     Rsp = Rsp * Rsp;
-    p.W = 1.0f - Rsp;
-    p.s = -mc3d_xm_logf(orc_rand_oc1(rx, ra));
+    p.W = (real)1 - Rsp;
+    p.s = -R_LOG(orc_rand_oc1(rx, ra));
     uint64_t q0 = orc_q(p.W);
     orc_derive(G, &p);
 
@@ -387,7 +418,7 @@ static void orc_photon(const orc_g *G, const orc_tab *P, int beam, int64_t max_s
     int chunk = 0;
     int64_t steps = 0;
     for (;;) {
-        float db;
+        real db;
         int froze = orc_step(G, P, &p, rx, ra, &killed, &created, &db, &fresnel, amap);
         chunk++;
         steps++;
@@ -395,15 +426,15 @@ static void orc_photon(const orc_g *G, const orc_tab *P, int beam, int64_t max_s
         if (froze) {
             /* the rest of the 45-step launch: masked steps (mirror + boundary distance) */
             for (int m = chunk; m < ORC_NUM_PHOTON_STEPS; m++) {
-                float nx_ = p.x, ny_ = p.y, nz_ = p.z;
+                real nx_ = p.x, ny_ = p.y, nz_ = p.z;
                 db = orc_intersection(G, p.i, p.j, p.k, &nx_, p.ux, &ny_, p.uy, &nz_, p.uz);
                 if (!orc_mirror(&p.x, &p.ux, G->Lx)) orc_mirror(&p.y, &p.uy, G->Ly);
             }
-            float wb = p.W;
+            real wb = p.W;
             if (orc_quickfix(&p, db)) { acc->t[12]++; lost = orc_q(wb); }
             done = 1;
         } else if (chunk == ORC_NUM_PHOTON_STEPS) {
-            float wb = p.W;
+            real wb = p.W;
             if (orc_quickfix(&p, db)) { acc->t[12]++; lost = orc_q(wb); done = 1; }
             else { orc_derive(G, &p); chunk = 0; }
         }
@@ -479,10 +510,18 @@ int orc_run(const orc_geom *geom, const orc_props *props, const orc_job *job,
     }
     orc_g G;
     G.nx = geom->nx; G.ny = geom->ny; G.nz = geom->nz;
-    G.dx = (float)geom->dx; G.dy = (float)geom->dy; G.dz = (float)geom->dz;
+    G.dx = (real)geom->dx; G.dy = (real)geom->dy; G.dz = (real)geom->dz;
     G.Lx = G.dx * G.nx; G.Ly = G.dy * G.ny; G.Lz = G.dz * G.nz;
     G.tissue = geom->tissue;
-    orc_tab P = {props->mua, props->mus, props->g, props->n};
+    /* optical properties in the transport type (the file values are float) */
+    real *tabv = (real *)malloc(sizeof(real) * 4 * (size_t)props->ntypes);
+    for (int t = 0; t < props->ntypes; t++) {
+        tabv[t] = props->mua[t];
+        tabv[props->ntypes + t] = props->mus[t];
+        tabv[2 * props->ntypes + t] = props->g[t];
+        tabv[3 * props->ntypes + t] = props->n[t];
+    }
+    orc_tab P = {tabv, tabv + props->ntypes, tabv + 2 * props->ntypes, tabv + 3 * props->ntypes};
     int64_t nb = (int64_t)G.nx * G.ny;
     int64_t per = job->photons / S, rem = job->photons % S;
     int64_t max_steps = job->max_steps > 0 ? job->max_steps : (1 << 24);
@@ -521,6 +560,7 @@ int orc_run(const orc_geom *geom, const orc_props *props, const orc_job *job,
     }
     free(sx);
     free(sa);
+    free(tabv);
     return 0;
 }
 

@@ -28,6 +28,21 @@ def test_fast_vs_exact_chi2(table):
         assert abs(total_z(fast.totals, exact.totals, key)) < 5
 
 
+def test_fast_vs_exact_pencil_chi2(table):
+    """pencil beam into a homogeneous slab: the radial fall-off of the DRS is steep,
+    so a bias of the fast path's crossing logic would show in the inner bins"""
+    g = m.Geometry(np.ones((48, 64, 64), np.uint8), 0.05, 0.05, 0.05)
+    p = m.OpticalProps.from_tissues([(0.02, 8.0, 0.9, 1.37)])
+    fast = m.run([g], [p], [m.Job(0, 0, 3_000_000, 11, "pencil")], table=table)[0]
+    exact = m.run([g], [p], [m.Job(0, 0, 3_000_000, 12, "pencil")], table=table,
+                  math="exact")[0]
+    chi2, dof, pv = drs_chi2(fast.drs, fast.drs_sq, fast.photons, exact.drs, exact.drs_sq,
+                             exact.photons, f=2)
+    assert dof > 100 and pv > 1e-4, (chi2, dof, pv)
+    for key in ("r_in", "r_out", "absorbed"):
+        assert abs(total_z(fast.totals, exact.totals, key)) < 5, key
+
+
 def test_fast_vs_oracle_chi2(table):
     g, p = m.Geometry(np.ones((32, 32, 32), np.uint8), 0.1, 0.1, 0.1), \
         m.OpticalProps.from_tissues([(0.05, 10.0, 0.9, 1.4)])
@@ -51,7 +66,8 @@ def test_conservation_exact(table):
     assert t["w_launched"] > 0 and t["steps"] > t["photons"]
 
 
-@pytest.mark.parametrize("block,bps", [(64, 1), (128, 3), (256, 0), (96, 2)])
+@pytest.mark.parametrize("block,bps", [(64, 1), (128, 3), (256, 0), (96, 2), (256, 4),
+                                       (128, 8)])
 def test_launch_shape_reproducible(table, block, bps):
     g, p = layered_small()
     job = m.Job(0, 0, 300_000, 4242, "uniform")
@@ -80,4 +96,31 @@ def test_plan_reexecute_identical(table):
     plan.execute()
     b = plan.read()[0]
     plan.close()
+    assert a.totals == b.totals and np.array_equal(a.drs, b.drs)
+
+
+def test_plan_graph_replay_identical(table):
+    """a plan captured into a CUDA graph replays to the same tallies"""
+    g, p = layered_small()
+    jobs = [m.Job(0, 0, 150_000, 9, "uniform"), m.Job(0, 0, 50_000, 10, "pencil")]
+    direct = m.run([g], [p], jobs, table=table)
+    plan = m.Plan([g], [p], jobs, table=table, use_graph=True)
+    for _ in range(3):
+        plan.execute()
+        got = plan.read()
+        for a, b in zip(got, direct):
+            assert a.totals == b.totals and np.array_equal(a.drs, b.drs)
+    plan.close()
+
+
+def test_autotune_picks_a_shape_and_results_stay(table):
+    from ymc3d_b200 import autotune
+    g, p = layered_small()
+    jobs = [m.Job(0, 0, 400_000, 31, "uniform")]
+    choice = autotune.tune([g], [p], jobs, table=table, use_cache=False,
+                           candidates=((256, 0), (128, 0), (64, 2)))
+    assert choice["block"] in (256, 128, 64) and len(choice["table"]) == 3
+    a = m.run([g], [p], jobs, table=table)[0]
+    b = m.run([g], [p], jobs, table=table, block=choice["block"],
+              blocks_per_sm=choice["blocks_per_sm"])[0]
     assert a.totals == b.totals and np.array_equal(a.drs, b.drs)

@@ -84,3 +84,17 @@ def test_stream_subsets_add_up(orc, table):
         assert np.array_equal(sum(q[k] for q in parts), whole[k])
     for k in whole["totals"]:
         assert sum(q["totals"][k] for q in parts) == whole["totals"][k]
+
+
+def test_oracle_regression_fixture(orc):
+    """the FP32 oracle still produces the pinned tallies and photon logs"""
+    import json
+    from pathlib import Path
+
+    import sys
+    sys.path.insert(0, str(Path(__file__).parent / "golden"))
+    import make_oracle_regression as mk
+    want = json.loads((Path(__file__).parent / "golden" / "oracle_regression.json").read_text())
+    table = m.safeprime_table(mk.TABLE_LINES)
+    for name, g, p, job in mk.cases():
+        assert mk.run_case(g, p, job, table) == want[name], name

@@ -32,7 +32,7 @@ BEAMS = {"uniform": 0, "pencil": 1}
 MATH = {"fast": 0, "exact": 1}
 TOTAL_FIELDS = ("photons", "steps", "w_launched", "r_in", "r_out", "t_in", "t_out", "absorbed",
                 "rr_killed", "rr_created", "lost", "capped", "quickfix", "fresnel")
-DEFAULT_STREAMS = 4194304
+DEFAULT_STREAMS = 1 << 40  # include/mc3d.h: one photon per stream unless a job says otherwise
 
 
 class Mc3dError(RuntimeError):
@@ -76,7 +76,7 @@ PHOTON_RECORD_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("ux",
 class COptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("math", C.c_int32), ("block", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("absorption_map", C.c_int32),
-                ("reserved", C.c_int32), ("max_steps", C.c_int64),
+                ("use_graph", C.c_int32), ("max_steps", C.c_int64),
                 ("photon_log", C.c_void_p), ("cancel", C.c_void_p)]
 
 
@@ -261,12 +261,13 @@ class Result:
 
 
 def _options(device=0, math="fast", block=0, blocks_per_sm=0, max_steps=0, log=None,
-             cancel=None, absorption_map=False) -> COptions:
+             cancel=None, absorption_map=False, use_graph=False) -> COptions:
     o = COptions()
     lib().mc3d_default_options(C.byref(o))
     o.device, o.math, o.block, o.blocks_per_sm, o.max_steps = (
         device, MATH[math], block, blocks_per_sm, max_steps)
     o.absorption_map = int(bool(absorption_map))
+    o.use_graph = int(bool(use_graph))
     o.photon_log = _ptr(log)
     o.cancel = _ptr(cancel)
     return o
@@ -327,11 +328,11 @@ class Plan:
     """Inputs resident on the device; execute() any number of times (mc3d_plan_*)."""
 
     def __init__(self, geoms, props, jobs, table=None, math="fast", device=0, block=0,
-                 blocks_per_sm=0, max_steps=0):
+                 blocks_per_sm=0, max_steps=0, use_graph=False):
         self.geoms, self.props, self.jobs = list(geoms), list(props), list(jobs)
         self.table = default_table() if table is None else np.ascontiguousarray(table, np.uint32)
         g, p, j = _arrays(self.geoms, self.props, self.jobs)
-        opt = _options(device, math, block, blocks_per_sm, max_steps)
+        opt = _options(device, math, block, blocks_per_sm, max_steps, use_graph=use_graph)
         self._h = C.c_void_p()
         _check(lib().mc3d_plan_create(C.byref(self._h), g, len(self.geoms), p, len(self.props),
                                       j, len(self.jobs), self.table.ctypes.data, len(self.table),

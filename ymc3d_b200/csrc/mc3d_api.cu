@@ -132,6 +132,7 @@ int list_rejections_host(const mc3d_seed_consts &sc, uint64_t seed, const uint32
 struct mc3d_plan {
     int device = 0;
     int math = MC3D_MATH_FAST;
+    int variant = 0; /* fast kernel register budget, see launch_photon_fast */
     int block = 256;
     int grid = 0;
     size_t smem = 0;
@@ -155,6 +156,9 @@ struct mc3d_plan {
     mc3d_photon_record *h_log = nullptr;
     volatile int32_t *h_cancel = nullptr;
     int *d_cancel = nullptr;
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
     bool cancel_registered = false;
     KernelParams P;
 };
@@ -176,6 +180,8 @@ static void plan_free(mc3d_plan *p)
     cudaFree(p->d_amap);
     cudaFree(p->d_log);
     if (p->cancel_registered) cudaHostUnregister((void *)p->h_cancel);
+    if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
     if (p->stream) cudaStreamDestroy(p->stream);
     cudaSetDevice(prev);
     delete p;
@@ -254,6 +260,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     p->njobs = njobs;
     p->h_log = opt.photon_log;
     p->h_cancel = opt.cancel;
+    p->use_graph = opt.use_graph != 0;
 
     std::vector<JobDev> jh(njobs);
     int64_t stream_base = 0, bin_base = 0, photon_base = 0, scan_base = 0, voxel_base = 0;
@@ -445,8 +452,15 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         PLAN_TRY(p->math == MC3D_MATH_FAST ? smem_limit_photon_fast(p->smem)
                                           : smem_limit_photon_exact(p->smem));
     }
+    /* four or more blocks of 256 per SM need the 64-register variant */
+    p->variant = (p->math == MC3D_MATH_FAST && !opt.absorption_map &&
+                  (int64_t)opt.blocks_per_sm * p->block >= 1024) ? 1 : 0;
+    /* experiment knob: the fast kernel on the reference-structured step */
+    const char *fs = getenv("MC3D_FAST_STEP");
+    if (p->math == MC3D_MATH_FAST && !opt.absorption_map && fs && !strcmp(fs, "reference"))
+        p->variant = 2;
     int bps = 0;
-    PLAN_TRY(p->math == MC3D_MATH_FAST ? occupancy_photon_fast(p->block, p->smem, &bps)
+    PLAN_TRY(p->math == MC3D_MATH_FAST ? occupancy_photon_fast(p->block, p->smem, &bps, p->variant)
                                       : occupancy_photon_exact(p->block, p->smem, &bps));
     if (bps <= 0) {
         plan_free(p);
@@ -482,17 +496,40 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
 #undef PLAN_TRY
 }
 
+/* clear the tallies and launch: the work of one execute, on stream s */
+static int plan_enqueue(mc3d_plan *p, cudaStream_t s)
+{
+    size_t tally_words = 3 * (size_t)p->total_bins + (size_t)p->njobs * MC3D_NUM_TOTALS + 1;
+    CUDA_TRY(cudaMemsetAsync(p->d_tally, 0, tally_words * sizeof(unsigned long long), s));
+    if (p->d_amap)
+        CUDA_TRY(cudaMemsetAsync(p->d_amap, 0, sizeof(unsigned long long) * p->total_voxels, s));
+    if (p->math == MC3D_MATH_FAST)
+        CUDA_TRY(launch_photon_fast(p->P, p->grid, p->block, p->smem, s, p->variant));
+    else CUDA_TRY(launch_photon_exact(p->P, p->grid, p->block, p->smem, s));
+    return MC3D_OK;
+}
+
 int mc3d_plan_execute(mc3d_plan *p, void *stream)
 {
     if (!p) return fail(MC3D_ERR_ARG, "plan is NULL");
     cudaStream_t s = stream ? (cudaStream_t)stream : p->stream;
     CUDA_TRY(cudaSetDevice(p->device));
-    size_t tally_words = 3 * (size_t)p->total_bins + (size_t)p->njobs * MC3D_NUM_TOTALS + 1;
-    CUDA_TRY(cudaMemsetAsync(p->d_tally, 0, tally_words * sizeof(unsigned long long), s));
-    if (p->d_amap)
-        CUDA_TRY(cudaMemsetAsync(p->d_amap, 0, sizeof(unsigned long long) * p->total_voxels, s));
-    if (p->math == MC3D_MATH_FAST) CUDA_TRY(launch_photon_fast(p->P, p->grid, p->block, p->smem, s));
-    else CUDA_TRY(launch_photon_exact(p->P, p->grid, p->block, p->smem, s));
+    if (!p->use_graph) return plan_enqueue(p, s);
+    if (!p->graph_exec) {
+        /* capture on the plan's own stream, then replay on any stream */
+        CUDA_TRY(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+        int st = plan_enqueue(p, p->stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+        if (st) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess) return fail(MC3D_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        p->graph = g;
+        CUDA_TRY(cudaGraphInstantiate(&p->graph_exec, p->graph, 0));
+    }
+    CUDA_TRY(cudaGraphLaunch(p->graph_exec, s));
     return MC3D_OK;
 }
 

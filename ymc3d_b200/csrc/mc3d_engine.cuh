@@ -331,6 +331,189 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     return freeze;
 }
 
+/* ------------------------------------------------------------ fast-math step
+ * The same physics as photon_step, organised for SIMT throughput:
+ *  - a face crossing only snaps, moves and looks up the next voxel.  The four
+ *    random numbers the reference draws on a crossing (roulette, two for the
+ *    Henyey-Greenstein spin, a new path length) are all discarded there, so
+ *    they are not drawn: the photon's statistics are unchanged while the random
+ *    stream is consumed only by the draws that decide something;
+ *  - cell indices move by one on the snapped axes; the other axes are kept when
+ *    the new position lies strictly inside the cell, and otherwise recomputed
+ *    with photontrack_get_grid_coord's rule;
+ *  - absorption, roulette, scattering and the new path length run only for the
+ *    lanes whose step ends in the tissue, behind one branch;
+ *  - a crossing without a Fresnel event keeps its direction unnormalised again.
+ * Returns true when the photon froze; *db receives the boundary distance. */
+template <bool AMAP>
+static __device__ __forceinline__ bool photon_step_fast(const GeomDev &g, const float4 *tab,
+                                                        Photon &p, uint64_t &rx, uint32_t ra,
+                                                        const Acc &acc, float *db_out,
+                                                        uint32_t *fresnel_count,
+                                                        unsigned long long *amap,
+                                                        bool *lat_mirror)
+{
+    typedef MathFast M;
+    const float4 t0 = tab[MC3D_TAB_STRIDE * p.tissue];
+    const float4 t1 = tab[MC3D_TAB_STRIDE * p.tissue + 1];
+    const float ni = t0.w;
+    const float mu_t = t1.x;
+
+    /* DDA to the next face, src/mc3d_gpu.cu:29-49 */
+    const int si = (p.ux >= 0) ? 1 : 0, sj = (p.uy >= 0) ? 1 : 0, sk = (p.uz >= 0) ? 1 : 0;
+    const float bx = (float)(p.i + si) * g.dx;
+    const float by = (float)(p.j + sj) * g.dy;
+    const float bz = (float)(p.k + sk) * g.dz;
+    const float tx = __fdividef(bx - p.x, p.ux);
+    const float ty = __fdividef(by - p.y, p.uy);
+    const float tz = __fdividef(bz - p.z, p.uz);
+    const float db = fminf(tx, fminf(ty, tz));
+    const bool hit = db * mu_t <= p.s;
+    const bool hx = hit && (db == tx), hy = hit && (db == ty), hz = hit && (db == tz);
+
+    /* new position: the face (snapped) or the interaction point s / mu_t away */
+    const float dist = hit ? db : p.s * t1.z;
+    float newx = hx ? bx : p.x + p.ux * dist;
+    float newy = hy ? by : p.y + p.uy * dist;
+    float newz = hz ? bz : p.z + p.uz * dist;
+    const float s_left = hit ? p.s - db * mu_t : 0.0f;
+
+    /* next cell: +-1 on a snapped axis, unchanged where strictly inside */
+    int nexti = hx ? p.i + 2 * si - 1 : p.i;
+    int nextj = hy ? p.j + 2 * sj - 1 : p.j;
+    int nextk = hz ? p.k + 2 * sk - 1 : p.k;
+    /* the cell's other face on each axis (the DDA border is the first) */
+    const float ox = (float)(p.i + 1 - si) * g.dx;
+    const float oy = (float)(p.j + 1 - sj) * g.dy;
+    const float oz = (float)(p.k + 1 - sk) * g.dz;
+    const bool okx = hx || (newx > fminf(bx, ox) && newx < fmaxf(bx, ox));
+    const bool oky = hy || (newy > fminf(by, oy) && newy < fmaxf(by, oy));
+    const bool okz = hz || (newz > fminf(bz, oz) && newz < fmaxf(bz, oz));
+    if (!(okx && oky && okz)) {
+        nexti = grid_coord<M>(newx, p.ux, g.dx, g.rdx);
+        nextj = grid_coord<M>(newy, p.uy, g.dy, g.rdy);
+        nextk = grid_coord<M>(newz, p.uz, g.dz, g.rdz);
+    }
+    int next_tissue = p.tissue;
+    if (nexti != p.i || nextj != p.j || nextk != p.k || newz <= 0)
+        next_tissue = tissue_at(g, nexti, nextj, nextk, newz, p.uz);
+
+    float W = p.W;
+    float nux = p.ux, nuy = p.uy, nuz = p.uz;
+    bool refl = false, renorm = false;
+    bool freeze = (mu_t == 0);
+    float s_new = s_left;
+    if (hit) {
+        const float nt = tab[MC3D_TAB_STRIDE * next_tissue].w;
+        if (ni != nt) { /* Fresnel, src/mc3d_gpu.cu:226-257 */
+            float cos_ai = (p.i != nexti) ? p.ux : ((p.j != nextj) ? p.uy : p.uz);
+            cos_ai = fabsf(cos_ai);
+            cos_ai = (cos_ai > 1) ? 1 : cos_ai;
+            float ai = acosf(cos_ai);
+            float ni_nt = M::div(ni, nt);
+            float sin_ai = sinf(ai);
+            float sin_at = ni_nt * sin_ai;
+            float cos_at = sqrtf(1.0f - sin_at * sin_at);
+            float R1 = M::div(sin_ai * cos_at - cos_ai * sin_at, sin_ai * cos_at + cos_ai * sin_at);
+            float R2 = M::div(cos_ai * cos_at - sin_ai * sin_at, cos_ai * cos_at + sin_at * sin_at);
+            float R = 0.5 * R1 * R1 * (1.0f + R2 * R2);
+            R = (sin_at > 1) ? 1 : R;
+            float eps = mc3d_rand_co(&rx, ra);
+            refl = eps < R;
+            nux = refl ? p.ux * ((p.i == nexti) ? 1 : -1)
+                       : ((p.i != nexti) ? copysignf(cos_at, p.ux * cos_at) : p.ux * ni_nt);
+            nuy = refl ? p.uy * ((p.j == nextj) ? 1 : -1)
+                       : (((p.j != nextj) && (p.i == nexti)) ? copysignf(cos_at, p.uy * cos_at)
+                                                             : p.uy * ni_nt);
+            nuz = refl ? p.uz * ((p.k == nextk) ? 1 : -1)
+                       : (((p.k != nextk) && (p.j == nextj) && (p.i == nexti))
+                              ? copysignf(cos_at, p.uz * cos_at)
+                              : p.uz * ni_nt);
+            renorm = true;
+            (*fresnel_count)++;
+        }
+    } else {
+        /* absorption, src/mc3d_gpu.cu:262-263 */
+        const float W_before = W;
+        if (mu_t > 0) W = W - t1.y * W;
+        if (AMAP && mu_t > 0) {
+            int ai = min(max(p.i, 0), g.nx - 1);
+            int aj = min(max(p.j, 0), g.ny - 1);
+            int ak = min(max(p.k, 0), g.nz - 1);
+            uint64_t dq = qw(W_before) - qw(W);
+            if (dq) atomicAdd(amap + ((int64_t)ak * g.ny + aj) * g.nx + ai, (unsigned long long)dq);
+        }
+        /* russian roulette, src/mc3d_gpu.cu:275-277 */
+        float eps = mc3d_rand_co(&rx, ra);
+        if ((W <= MC3D_W_THRESHOLD_LE_F) && (mu_t != 0)) {
+            float newW = (eps < MC3D_SURVIVAL_LT_F) ? (float)((double)W / MC3D_SURVIVAL_CHANCE)
+                                                     : 0.0f;
+            if (newW == 0.0f) {
+                uint64_t k = qw(W);
+                acc[T_RR_KILLED] += k;
+                acc[T_ABSORBED] -= k;
+            } else {
+                uint64_t c = qw(newW) - qw(W);
+                acc[T_RR_CREATED] += c;
+                acc[T_ABSORBED] += c;
+            }
+            W = newW;
+        }
+        /* Henyey-Greenstein, src/mc3d_gpu.cu:282-294 */
+        const float4 t2 = tab[MC3D_TAB_STRIDE * p.tissue + 2];
+        float costheta = M::div(t2.x, t2.y + t2.z * mc3d_rand_oc(&rx, ra));
+        costheta = t1.w * (t2.w - costheta * costheta);
+        float sintheta = sqrtf(1 - costheta * costheta);
+        float cosphi, sinphi;
+        M::sincospi(2 * mc3d_rand_co(&rx, ra), &sinphi, &cosphi);
+        const float one_uz2 = 1 - p.uz * p.uz;
+        const float invsqrt = rsqrtf(one_uz2);
+        const bool steep = !(fabsf(p.uz) <= MC3D_UZ_THRESH_LE_F);
+        nux = !steep ? sintheta * (p.ux * p.uz * cosphi - p.uy * sinphi) * invsqrt +
+                           p.ux * costheta
+                     : sintheta * cosphi;
+        nuy = !steep ? sintheta * (p.uy * p.uz * cosphi + p.ux * sinphi) * invsqrt +
+                           p.uy * costheta
+                     : sintheta * sinphi;
+        nuz = !steep ? -one_uz2 * invsqrt * sintheta * cosphi + p.uz * costheta
+                     : copysignf(costheta, costheta * p.uz);
+        renorm = true;
+        freeze = freeze || (W <= 0);
+        /* new path length, src/mc3d_gpu.cu:319-321 */
+        const float e2 = mc3d_rand_oc(&rx, ra);
+        s_new = (W > 0) ? -__logf(e2) : 0;
+    }
+    if (renorm) {
+        const float zero_thresh = (float)(1 - MC3D_UZ_THRESH);
+        nux = (fabsf(nux) < zero_thresh) ? 0 : nux;
+        nuy = (fabsf(nuy) < zero_thresh) ? 0 : nuy;
+        nuz = (fabsf(nuz) < zero_thresh) ? 0 : nuz;
+        float norm = rsqrtf(nux * nux + nuy * nuy + nuz * nuz);
+        nux *= norm;
+        nuy *= norm;
+        nuz *= norm;
+    }
+    p.W = W;
+    if (!freeze) {
+        p.ux = nux; p.uy = nuy; p.uz = nuz;
+        p.x = newx; p.y = newy; p.z = newz;
+        p.s = s_new;
+    } else {
+        p.s = s_left;
+    }
+    /* mirror, short-circuited by a Fresnel reflection (src/mc3d_gpu.cu:330) */
+    const bool fres_refl = refl;
+    if (!(p.x > 0 && p.x < g.Lx && p.y > 0 && p.y < g.Ly))
+        refl = refl || mirror(&p.x, &p.ux, g.Lx) || mirror(&p.y, &p.uy, g.Ly);
+    *lat_mirror = refl && !fres_refl;
+    if (!((hit && refl) || freeze)) {
+        p.i = nexti; p.j = nextj; p.k = nextk;
+        p.tissue = next_tissue;
+    }
+    *db_out = db;
+    return freeze;
+}
+
 /* i, j, k and tissue from the position, as at the start of every launch of
  * photontrack_step (src/mc3d_gpu.cu:168-171). */
 template <class M>
@@ -425,7 +608,9 @@ static __device__ __forceinline__ uint64_t stream_seed(const KernelParams &P, co
     return mc3d_seed_attempt(xs, P.seed.begin, fora);
 }
 
-template <class M, bool AMAP>
+/* SPLIT selects photon_step_fast for the fast policy (the default); false runs
+ * the reference-structured photon_step with fast math (an experiment variant) */
+template <class M, bool AMAP, bool SPLIT = true>
 __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
 {
     extern __shared__ float4 sh_tab[];
@@ -495,8 +680,13 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
 
         float db;
         bool lat_mirror;
-        bool froze = photon_step<M, AMAP>(g, tab, p, rx, ra, acc, &db, &fresnel, amap,
-                                          &lat_mirror);
+        bool froze;
+        if constexpr (M::kFast && SPLIT)
+            froze = photon_step_fast<AMAP>(g, tab, p, rx, ra, acc, &db, &fresnel, amap,
+                                           &lat_mirror);
+        else
+            froze = photon_step<M, AMAP>(g, tab, p, rx, ra, acc, &db, &fresnel, amap,
+                                         &lat_mirror);
         chunk++;
         psteps++;
 

@@ -11,11 +11,13 @@
 
 namespace mc3d {
 
+/* variant 0: 80-register budget (3 blocks of 256 per SM); 1: 64 registers (4 blocks);
+ * 2: the reference-structured step with fast math (A/B experiments) */
 cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_t smem,
-                               cudaStream_t stream);
+                               cudaStream_t stream, int variant);
 cudaError_t launch_photon_exact(const KernelParams &P, int grid, int block, size_t smem,
                                 cudaStream_t stream);
-cudaError_t occupancy_photon_fast(int block, size_t smem, int *blocks_per_sm);
+cudaError_t occupancy_photon_fast(int block, size_t smem, int *blocks_per_sm, int variant);
 cudaError_t occupancy_photon_exact(int block, size_t smem, int *blocks_per_sm);
 cudaError_t smem_limit_photon_fast(size_t smem);
 cudaError_t smem_limit_photon_exact(size_t smem);
