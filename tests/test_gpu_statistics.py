@@ -124,3 +124,18 @@ def test_autotune_picks_a_shape_and_results_stay(table):
     b = m.run([g], [p], jobs, table=table, block=choice["block"],
               blocks_per_sm=choice["blocks_per_sm"])[0]
     assert a.totals == b.totals and np.array_equal(a.drs, b.drs)
+
+
+def test_cancel_flag_stops_and_keeps_partial_tallies_consistent(table):
+    """the host-side stop (the reference stops on SIGINT, src/mc3d_gpu.cu:379-394,
+    573-577): a flag set before the launch makes every thread stop at its first
+    stream; the call reports MC3D_ERR_CANCELLED and the partial tallies still
+    conserve weight exactly"""
+    g, p = layered_small()
+    flag = np.array([1], np.int32)
+    with pytest.raises(m.Mc3dError) as e:
+        m.run([g], [p], [m.Job(0, 0, 500_000, 3, "uniform")], table=table, cancel=flag)
+    assert e.value.status == -12
+    part = e.value.results[0]
+    assert part.photons < 500_000
+    assert part.conservation_residual() == 0

@@ -310,17 +310,27 @@ def _finish(res, outs, jobs, log):
 def run(geoms: Sequence[Geometry], props: Sequence[OpticalProps], jobs: Sequence[Job],
         table: np.ndarray | None = None, math: str = "fast", device: int = 0, block: int = 0,
         blocks_per_sm: int = 0, max_steps: int = 0, photon_log: bool = False,
-        absorption_map: bool = False) -> list[Result]:
-    """Run every job in one persistent launch (mc3d_run)."""
+        absorption_map: bool = False, cancel: np.ndarray | None = None) -> list[Result]:
+    """Run every job in one persistent launch (mc3d_run).  `cancel`, an int32 array
+    of one element, is read by the kernel whenever a thread takes a new stream: set
+    it non-zero (from another thread) to stop; the call then raises
+    MC3D_ERR_CANCELLED and the partial results are in the exception's .results."""
     table = default_table() if table is None else np.ascontiguousarray(table, dtype=np.uint32)
     g, p, j = _arrays(geoms, props, jobs)
     res, outs = _outs(geoms, jobs, absorption_map)
     log = (np.zeros(sum(int(x.photons) for x in jobs), PHOTON_RECORD_DTYPE)
            if photon_log else None)
+    if cancel is not None:
+        cancel = np.ascontiguousarray(cancel, np.int32)
     opt = _options(device, math, block, blocks_per_sm, max_steps, log,
-                   absorption_map=absorption_map)
-    _check(lib().mc3d_run(g, len(geoms), p, len(props), j, len(jobs), table.ctypes.data,
-                          len(table), C.byref(opt), outs))
+                   absorption_map=absorption_map, cancel=cancel)
+    st = lib().mc3d_run(g, len(geoms), p, len(props), j, len(jobs), table.ctypes.data,
+                        len(table), C.byref(opt), outs)
+    if st == -12:
+        err = Mc3dError(st, lib().mc3d_last_error().decode(errors="replace"))
+        err.results = _finish(res, outs, jobs, log)
+        raise err
+    _check(st)
     return _finish(res, outs, jobs, log)
 
 

@@ -455,9 +455,9 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     /* four or more blocks of 256 per SM need the 64-register variant */
     p->variant = (p->math == MC3D_MATH_FAST && !opt.absorption_map &&
                   (int64_t)opt.blocks_per_sm * p->block >= 1024) ? 1 : 0;
-    /* experiment knob: the fast kernel on the reference-structured step */
+    /* experiment knob: the fast kernel on the split step (photon_step_fast) */
     const char *fs = getenv("MC3D_FAST_STEP");
-    if (p->math == MC3D_MATH_FAST && !opt.absorption_map && fs && !strcmp(fs, "reference"))
+    if (p->math == MC3D_MATH_FAST && !opt.absorption_map && fs && !strcmp(fs, "split"))
         p->variant = 2;
     int bps = 0;
     PLAN_TRY(p->math == MC3D_MATH_FAST ? occupancy_photon_fast(p->block, p->smem, &bps, p->variant)

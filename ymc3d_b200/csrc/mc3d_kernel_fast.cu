@@ -27,11 +27,11 @@ __global__ void __launch_bounds__(256, 4)
     photon_kernel_body<MathFast, false>(P);
 }
 
-/* the reference-structured step with fast math, for A/B measurements */
+/* the split step (photon_step_fast), kept for A/B measurements */
 __global__ void __launch_bounds__(256, 3)
-    photon_kernel_fast_refstep(const __grid_constant__ KernelParams P)
+    photon_kernel_fast_split(const __grid_constant__ KernelParams P)
 {
-    photon_kernel_body<MathFast, false, false>(P);
+    photon_kernel_body<MathFast, false, true>(P);
 }
 
 cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_t smem,
@@ -39,7 +39,7 @@ cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_
 {
     if (P.amap) photon_kernel_fast_amap<<<grid, block, smem, stream>>>(P);
     else if (variant == 1) photon_kernel_fast_r64<<<grid, block, smem, stream>>>(P);
-    else if (variant == 2) photon_kernel_fast_refstep<<<grid, block, smem, stream>>>(P);
+    else if (variant == 2) photon_kernel_fast_split<<<grid, block, smem, stream>>>(P);
     else photon_kernel_fast<<<grid, block, smem, stream>>>(P);
     return cudaGetLastError();
 }
@@ -61,7 +61,7 @@ cudaError_t smem_limit_photon_fast(size_t smem)
     e = cudaFuncSetAttribute(photon_kernel_fast_r64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(photon_kernel_fast_refstep,
+    e = cudaFuncSetAttribute(photon_kernel_fast_split,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(photon_kernel_fast_amap,

@@ -12,7 +12,7 @@
 namespace mc3d {
 
 /* variant 0: 80-register budget (3 blocks of 256 per SM); 1: 64 registers (4 blocks);
- * 2: the reference-structured step with fast math (A/B experiments) */
+ * 2: the split step photon_step_fast (A/B experiments) */
 cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_t smem,
                                cudaStream_t stream, int variant);
 cudaError_t launch_photon_exact(const KernelParams &P, int grid, int block, size_t smem,
