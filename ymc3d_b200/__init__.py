@@ -18,7 +18,9 @@ from typing import Sequence
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-LIB_PATH = HERE / "libmc3d.so"
+# MC3D_LIBRARY points the package at another build of the library (debug builds,
+# A/B measurements); the default is the in-tree build
+LIB_PATH = Path(os.environ.get("MC3D_LIBRARY", HERE / "libmc3d.so"))
 WEIGHT_SCALE = 4294967296.0  # fixed point: Q(W) = round(W * 2^32)
 
 MC3D_OK = 0
