@@ -42,3 +42,36 @@ def test_writers_round_trip(engine, tmp_path):
     p = engine.opticalprops_read_from_file(tmp_path / "p.bid")
     assert np.allclose(p.mua[1:], [r[0] for r in W.LAYER_ROWS])
     assert p.n[0] == 1.0 and p.mua[0] == 0
+
+
+def test_read_property_file_2d_and_3d(engine, tmp_path):
+    rng = np.random.default_rng(9)
+    a2 = rng.uniform(size=(5, 7))
+    engine.lib().mc3d_save_property(str(tmp_path / "a.bin").encode(), 2, 7, 5, 1, 0.1, 0.2, 0.0,
+                                    a2.ctypes.data)
+    d, dx, dy, dz = W.read_property_file(tmp_path / "a.bin")
+    assert np.array_equal(d, a2) and (dx, dy, dz) == (0.1, 0.2, 0.0)
+    a3 = np.ascontiguousarray(rng.uniform(size=(3, 5, 7)))
+    engine.lib().mc3d_save_property(str(tmp_path / "b.bin").encode(), 3, 7, 5, 3, 0.1, 0.2, 0.3,
+                                    a3.ctypes.data)
+    d, dx, dy, dz = W.read_property_file(tmp_path / "b.bin")
+    assert np.array_equal(d, a3) and dz == 0.3
+    (tmp_path / "c.bin").write_bytes((tmp_path / "b.bin").read_bytes()[:-9])
+    import pytest
+    with pytest.raises(ValueError):
+        W.read_property_file(tmp_path / "c.bin")
+
+
+def test_skin_model_matches_the_matlab_recipe():
+    g = W.skin_geometry()
+    nx, ny, nz = g.shape
+    assert (nx, ny, nz) == (50, 50, 85)
+    col = g.tissue[:, 0, 0]
+    # epidermis 0.1 mm = 5 voxels, papillary 10 % of 1.5 mm = 7, reticular 67
+    assert np.all(col[:5] == 1) and np.all(col[5:12] == 2) and np.all(col[12:79] == 3)
+    assert np.all(col[79:] == 4)
+    assert (g.tissue == 5).sum() > 0 and np.all(g.tissue[:, 0, :] == g.tissue[:, -1, :])
+    p = W.skin_optprops(600.0, lambda oxy, lam: 1e4 * (1 + oxy))
+    assert p.num_tissue_types == 6
+    assert abs(p.g[1] - (0.62 + 600 * 29e-5)) < 1e-6
+    assert p.mua[5] > p.mua[3] > 0 and np.all(p.n[1:] == np.float32(1.4))

@@ -50,14 +50,77 @@ def write_optprops_file(path: str | os.PathLike, rows) -> None:
         rows.tofile(f)
 
 
+def read_property_file(path: str | os.PathLike):
+    """Any save_property file (src/mc3d_io.cu:175-216): outname_drs.bin,
+    _trans.bin (2 dims) or _abs.bin / _flu.bin (3 dims).  Returns (data, dx, dy,
+    dz) with data [ny, nx] or [nz, ny, nx] (x fastest on disk) -- what
+    matlab/read/read_general_mcfile.m returns, in C order; dz is 0 for 2 dims."""
+    raw = open(path, "rb").read()
+    dims = int(np.frombuffer(raw, "<i4", 1)[0])
+    if dims not in (2, 3):
+        raise ValueError(f"{path}: {dims} dimensions")
+    n = [int(v) for v in np.frombuffer(raw, "<i4", dims, offset=4)]
+    off = 4 + 4 * dims
+    d = [float(v) for v in np.frombuffer(raw, "<f8", dims, offset=off)]
+    off += 8 * dims
+    count = int(np.prod(n))
+    if len(raw) < off + 8 * count:
+        raise ValueError(f"{path}: truncated")
+    data = np.frombuffer(raw, "<f8", count, offset=off).reshape(n[::-1]).copy()
+    return data, d[0], d[1], (d[2] if dims == 3 else 0.0)
+
+
 def read_drs_file(path: str | os.PathLike) -> tuple[np.ndarray, float, float]:
     """outname_drs.bin (save_property with 2 dims, src/mc3d_io.cu:175-216)."""
-    raw = open(path, "rb").read()
-    dims, nx, ny = np.frombuffer(raw, "<i4", 3)
-    assert dims == 2
-    dx, dy = np.frombuffer(raw, "<f8", 2, offset=12)
-    data = np.frombuffer(raw, "<f8", int(nx) * int(ny), offset=28).reshape(int(ny), int(nx))
-    return data.copy(), float(dx), float(dy)
+    data, dx, dy, dz = read_property_file(path)
+    if data.ndim != 2:
+        raise ValueError(f"{path}: not a 2-D file")
+    return data, dx, dy
+
+
+# ------------------------------------------------------------------ skin model
+def skin_geometry(dx: float = 0.02, length_xy: float = 1.0, length_z: float = 1.7,
+                  epi: float = 0.1, dermis: float = 1.5, papillary_frac: float = 0.1,
+                  vessel_radius: float = 0.06, vessel_depth: float = 0.25) -> Geometry:
+    """The example model of matlab/geometry/prepare_geometry.m:2-55: epidermis,
+    papillary and reticular dermis, subcutis, and a blood vessel along y at half
+    the width.  Tissue indices 1..5 (file values 0..4 there, vessel 5 -> 6 here
+    is folded to index 5: epidermis 1, papillary 2, reticular 3, subcutis 4,
+    vessel 5).  As in the script, voxel n (1-based) is tested at n * dx."""
+    nx = ny = int(round(length_xy / dx))
+    nz = int(round(length_z / dx))
+    epi_vox = int(np.floor(epi / dx))
+    pap_vox = epi_vox + int(np.floor(papillary_frac * dermis / dx))
+    ret_vox = pap_vox + int(np.floor((1 - papillary_frac) * dermis / dx))
+    k = np.arange(nz)
+    layer = np.where(k < epi_vox, 1, np.where(k < pap_vox, 2, np.where(k < ret_vox, 3, 4)))
+    t = np.broadcast_to(layer.astype(np.uint8)[:, None, None], (nz, ny, nx)).copy()
+    xi = (np.arange(nx) + 1) * dx
+    zk = (np.arange(nz) + 1) * dx
+    vessel = ((xi[None, :] - length_xy / 2) ** 2 + (zk[:, None] - vessel_depth) ** 2
+              <= vessel_radius ** 2)
+    t[np.broadcast_to(vessel[:, None, :], t.shape)] = 5
+    return Geometry(t, dx, dx, dx)
+
+
+def skin_optprops(lam: float, mua_blood) -> OpticalProps:
+    """Optical properties of prepare_optprops.m:29-51 at wavelength `lam` (nm), in
+    1/mm, for skin_geometry's tissues.  mua_blood(oxygenation, lam) is the whole-
+    blood absorption in 1/m; the reference reads it from muab.mat, which it does
+    not distribute, so the caller supplies it.  The subcutis and vessel rows are
+    not in the script (its example is explicitly incomplete); they take the
+    reticular dermis values and whole blood at oxygenation 0.8, g 0.98."""
+    melanin = (lam / 694.0) ** -3.46
+    musr = 100 * (18.780 * (lam / 500.0) ** -0.22 + 17.6 * (lam / 500.0) ** -4)
+    g = 0.62 + lam * 29e-5
+    mus = musr / (1 - g) * 0.01
+    rows = [((227 * melanin + 0.002 * mua_blood(0.5, lam) + (1 - 0.01 - 0.002) * 25) * 0.01,
+             mus, g, 1.4),
+            ((0.01 * mua_blood(0.5, lam) + (1 - 0.01) * 25) * 0.01, mus, g, 1.4),
+            ((0.01 * mua_blood(0.8, lam) + (1 - 0.01) * 25) * 0.01, mus, g, 1.4),
+            ((0.01 * mua_blood(0.8, lam) + (1 - 0.01) * 25) * 0.01, mus, g, 1.4),
+            (mua_blood(0.8, lam) * 0.01, mus, 0.98, 1.4)]
+    return OpticalProps.from_tissues(rows)
 
 
 # ------------------------------------------------------------------ workloads
