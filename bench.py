@@ -40,8 +40,15 @@ sys.path.insert(0, str(ROOT))
 # sincospif); a Fresnel event (:226-257) adds 37, 6 of them special (acos, sin,
 # sqrt, 3 divisions).  The per-term breakdown is in DESIGN.md.
 OPS_STEP, SFU_STEP = 152, 20
+# a merged step adds the jump: radius x unit, compare, 3 x (x + u R)
+OPS_JUMP = 8
 OPS_FRESNEL, SFU_FRESNEL = 37, 6
 FP32_LANES_PER_SM, SFU_LANES_PER_SM = 128, 16
+# DRAM bytes read + written by one photon-kernel launch of the layered workload
+# (ncu dram__bytes_read.sum + dram__bytes_write.sum = 13,825,792 + 1,181,952 on a
+# 1e7-photon launch, profiles/photon_kernel_fast_layered_vessel_1e7_full.md): the
+# first touch of grid, table and tallies, independent of the photon count
+TRAFFIC_BYTES_PER_LAUNCH = 15_007_744
 
 
 def parse():
@@ -58,6 +65,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--step-mode", default="merged", choices=["merged", "voxel"],
+                    help="fast math: merged crossings in uniform tissue, or one step per voxel face")
     ap.add_argument("--workload", default="layered",
                     choices=["layered", "homogeneous", "sweep", "uneven", "deep"],
                     help="layered is the headline; the others are the batched and "
@@ -205,8 +214,9 @@ def run_ours(args):
     if not args.no_tune:
         from ymc3d_b200 import autotune
         tuned = autotune.tune([geom], w.props, [shard(warm_job)], table=table_p, math=args.math,
-                              device=dev, use_cache=False)
-    shape = {"block": tuned["block"], "blocks_per_sm": tuned["blocks_per_sm"]}
+                              device=dev, use_cache=False, steps=args.step_mode)
+    shape = {"block": tuned["block"], "blocks_per_sm": tuned["blocks_per_sm"],
+             "steps": args.step_mode}
     plan = m.Plan([geom], w.props, [shard(job)], table=table_p, math=args.math, device=dev,
                   **shape)
     warm_plan = m.Plan([geom], w.props, [shard(warm_job)], table=table_p, math=args.math,
@@ -306,16 +316,11 @@ def run_ours(args):
     steps_per_s = steps_tot / args.steps / world / t_step  # per GPU
     fres_per_s = fresnel_tot / args.steps / world / t_step
     sfu_ops = steps_per_s * SFU_STEP + fres_per_s * SFU_FRESNEL
-    fp32_ops = steps_per_s * (OPS_STEP - SFU_STEP) + fres_per_s * (OPS_FRESNEL - SFU_FRESNEL)
+    ops_step = OPS_STEP + (OPS_JUMP if args.math == "fast" and args.step_mode == "merged" else 0)
+    fp32_ops = steps_per_s * (ops_step - SFU_STEP) + fres_per_s * (OPS_FRESNEL - SFU_FRESNEL)
     sfu_peak = sms * SFU_LANES_PER_SM * f_max
     fp32_peak = sms * FP32_LANES_PER_SM * f_max
-    traffic = None
-    tp = ROOT / "profiles" / "traffic.json"
-    if tp.exists():
-        try:
-            traffic = json.loads(tp.read_text()).get("bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = TRAFFIC_BYTES_PER_LAUNCH
     block, grid, smem = plan.shape()
     line = {
         "metric": "photons/s (layered tissue + vessel, 256x256x128, uniform beam, 1 B200)",
@@ -327,7 +332,8 @@ def run_ours(args):
                    "photons_per_step": int(photons_step),
                    "step": "one launch of the whole job (each rank: its stream shard)",
                    "warmup": "3 launches of the same workload at a tenth of the photons", "voxels": list(g.shape), "voxel_mm": g.dx,
-                   "beam": "uniform", "math": args.math, "streams": S,
+                   "beam": "uniform", "math": args.math, "step_mode": args.step_mode,
+                   "streams": S,
                    "launch": {"block": block, "grid": grid, "smem": smem,
                               "autotuner": [{k: r[k] for k in ("block", "blocks_per_sm", "ms")}
                                             for r in tuned["table"]]},
@@ -340,10 +346,10 @@ def run_ours(args):
                                    f"{f_max / 1e6:.0f} MHz (MEASURED_PEAKS.json clock)",
                      "fp32": {"achieved": fp32_ops / 1e9, "peak": fp32_peak / 1e9,
                               "frac": fp32_ops / fp32_peak},
-                     "ops_per_step": {"all": OPS_STEP, "sfu": SFU_STEP,
+                     "ops_per_step": {"all": ops_step, "sfu": SFU_STEP,
                                       "fresnel_all": OPS_FRESNEL, "fresnel_sfu": SFU_FRESNEL}},
         "clocks": clk,
-        "gpu_launches": launches * 2,
+        "gpu_launches": launches,  # one photon-kernel launch per step (after a tally memset)
         "e2e": e2e,
     }
     if not args.no_cpu_baseline:
@@ -490,7 +496,7 @@ def run_batched(args):
         return sum(ts) / len(ts), res
 
     with ClockSampler(dev) as clocks:
-        plan = m.Plan(w.geoms, w.props, w.jobs, math=args.math, device=dev)
+        plan = m.Plan(w.geoms, w.props, w.jobs, math=args.math, device=dev, steps=args.step_mode)
         t_batch, res = timed(plan, args.steps, args.warmup)
         plan.close()
         photons = sum(r.photons for r in res)
@@ -501,7 +507,7 @@ def run_batched(args):
             for job in w.jobs:
                 pl = m.Plan([w.geoms[job.geom]], [w.props[job.props]],
                             [m.Job(0, 0, job.photons, job.seed, job.beam)], math=args.math,
-                            device=dev)
+                            device=dev, steps=args.step_mode)
                 t, _ = timed(pl, 1, 1)
                 t_plain += t
                 pl.close()
@@ -513,7 +519,8 @@ def run_batched(args):
             "ms_per_step": t_batch * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+u64", "data": "synthetic (seeded)",
             "config": {"workload": w.name, "jobs": len(w.jobs), "photons_per_step": photons,
-                       "math": args.math, "photon_scale": args.photon_scale},
+                       "math": args.math, "step_mode": args.step_mode,
+                       "photon_scale": args.photon_scale},
             "steps_per_s": steps / t_batch, "plain": plain, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
 

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define MC3D_ABI_VERSION 1
+#define MC3D_ABI_VERSION 2
 #define MC3D_WEIGHT_SCALE 4294967296.0 /* 2^32: fixed-point units per unit weight */
 
 enum mc3d_status {
@@ -47,6 +47,15 @@ enum mc3d_status {
 
 enum mc3d_beam { MC3D_BEAM_UNIFORM = 0, MC3D_BEAM_PENCIL = 1 };
 enum mc3d_math { MC3D_MATH_FAST = 0, MC3D_MATH_EXACT = 1 };
+
+/* Step decomposition of the fast-math kernel.  MERGED (the default) replaces the
+ * voxel-face crossings of a flight through uniform tissue by one step to the
+ * edge of a sphere known to hold only that tissue (a per-voxel safe-distance
+ * map, built when the plan is created); each replaced crossing would only have
+ * moved the photon.  VOXEL steps at every voxel face, as the reference does
+ * (src/mc3d_gpu.cu:181-339).  Both are the reference's physics; the step counts
+ * in mc3d_totals differ.  Exact math always steps at every face. */
+enum mc3d_steps { MC3D_STEPS_MERGED = 0, MC3D_STEPS_VOXEL = 1 };
 
 /* Voxel geometry (geometry_t, src/mc3d_types.h:38-43), tissue indices as uint8
  * after the reader's +1 remap (0 = air). */
@@ -133,6 +142,8 @@ typedef struct {
     int64_t max_steps;      /* per-photon step cap, 0 = 2^24 */
     mc3d_photon_record *photon_log; /* host, sum of photons over jobs, or NULL */
     volatile int32_t *cancel;       /* optional host flag, read when a stream starts */
+    int32_t steps;                  /* enum mc3d_steps (fast math only) */
+    int32_t pad;
 } mc3d_options;
 
 /* ------------------------------------------------------------------ engine */
@@ -172,6 +183,15 @@ int mc3d_stream_seeds(const mc3d_job *job, const uint32_t *table, int64_t table_
  * on the GPU: out[g * n + d] for generator g of ngen with states x[g], a[g]. */
 int mc3d_mwc_draws(const uint64_t *x, const uint32_t *a, int64_t ngen, int64_t n, float *out,
                    int32_t device);
+
+/* No counterpart in the reference: the safe-distance map behind MC3D_STEPS_MERGED,
+ * computed on the GPU from a host grid (for tests).  radius holds nz + 63 slices
+ * of nx * ny (x fastest): slices below the grid stand for the medium's
+ * continuation there (the voxel index is clamped).  radius[v] is the largest
+ * r <= 63 such that every voxel within Chebyshev distance r of v has v's tissue
+ * and lies below the top face and inside the lateral faces. */
+int mc3d_safe_distance(const uint8_t *tissue, int32_t nx, int32_t ny, int32_t nz,
+                       uint8_t *radius, int32_t device);
 
 /* ------------------------------------------------- allocation-free entry point */
 

@@ -52,3 +52,26 @@ def total_z(ta: dict, tb: dict, key="r_in"):
     va = fa * (1 - min(fa, 1)) / ta["photons"] + 1e-30
     vb = fb * (1 - min(fb, 1)) / tb["photons"] + 1e-30
     return (fa - fb) / np.sqrt(va + vb)
+
+
+def safe_distance_bruteforce(t: np.ndarray, cap: int = 63) -> np.ndarray:
+    """Definition of the merged-step safe-distance map, checked cube by cube: on
+    the grid extended below by copies of its last slice (the clamped
+    continuation), per voxel the largest r <= cap such that the Chebyshev cube of
+    half-width r is uniform, below the top face and inside the lateral faces."""
+    from scipy.ndimage import maximum_filter, minimum_filter
+    nz, ny, nx = t.shape
+    ext = np.concatenate([t, np.repeat(t[-1:], cap, axis=0)]).astype(np.int16)
+    k, j, i = np.meshgrid(np.arange(nz + cap), np.arange(ny), np.arange(nx), indexing="ij")
+    out = np.zeros(ext.shape, np.uint8)
+    alive = np.ones(ext.shape, bool)
+    for q in range(1, cap + 1):
+        size = 2 * q + 1
+        inside = (k - q >= 0) & (j - q >= 0) & (i - q >= 0) & (j + q < ny) & (i + q < nx)
+        uniform = (maximum_filter(ext, size, mode="nearest") ==
+                   minimum_filter(ext, size, mode="nearest"))
+        alive &= inside & uniform
+        if not alive.any():
+            break
+        out[alive] = q
+    return out

@@ -31,7 +31,7 @@ def test_every_declared_symbol_is_exported(engine):
     lib = C.CDLL(str(engine.LIB_PATH))
     for n in names:
         getattr(lib, n)
-    assert lib.mc3d_abi_version() == 1
+    assert lib.mc3d_abi_version() == 2
 
 
 def _inputs(engine):
@@ -73,6 +73,12 @@ def test_host_side_validation(engine, table):
     assert _status(engine, lambda: run([g], big, [J(photons=10)], table)) == -11
     if not has_gpu():
         assert _status(engine, lambda: run([g], [p], [J(photons=10)], table)) == -8
+    opt = engine._options()
+    opt.steps = 7  # neither MC3D_STEPS_MERGED nor MC3D_STEPS_VOXEL
+    gg, pp, jj = engine._arrays([g], [p], [J(photons=10)])
+    _, outs = engine._outs([g], [J(photons=10)])
+    assert engine.lib().mc3d_run(gg, 1, pp, 1, jj, 1, table.ctypes.data, len(table),
+                                 C.byref(opt), outs) == -1
 
 
 def test_reference_shaped_entry_needs_table(engine, tmp_path, monkeypatch):

@@ -1,0 +1,108 @@
+"""Merged steps (MC3D_STEPS_MERGED, the fast-math default): the safe-distance map
+against its brute-force definition, and merged against per-face stepping on the
+same physics -- statistically equal tallies, exact conservation, fewer steps."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import ymc3d_b200 as m
+from helpers import drs_chi2, residual, safe_distance_bruteforce, total_z
+
+pytestmark = pytest.mark.gpu
+
+
+def _grids():
+    rng = np.random.default_rng(5)
+    yield np.ones((1, 1, 1), np.uint8)
+    yield np.ones((3, 1, 7), np.uint8)
+    yield np.ones((20, 18, 22), np.uint8)
+    blocky = np.kron(rng.integers(1, 4, (3, 4, 3)), np.ones((6, 5, 7), np.int64)).astype(np.uint8)
+    yield blocky
+    speckled = np.ones((16, 24, 20), np.uint8)
+    speckled[rng.random(speckled.shape) < 0.01] = 2
+    yield speckled
+    from ymc3d_b200.workloads import layered_vessel_geometry
+    yield layered_vessel_geometry(40, 36, 30, 0.08).tissue
+
+
+@pytest.mark.parametrize("k", range(6))
+def test_safe_distance_matches_definition(engine, k):
+    t = list(_grids())[k]
+    assert np.array_equal(m.safe_distance(t), safe_distance_bruteforce(t))
+
+
+def test_safe_distance_cap(engine):
+    t = np.ones((140, 140, 140), np.uint8)
+    r = m.safe_distance(t)
+    assert r.shape == (140 + 63, 140, 140)
+    assert r.max() == 63 and r[70, 70, 70] == 63 and r[200, 70, 70] == 63
+    assert r[0].max() == 0 and r[5, 70, 70] == 5 and r[70, 70, 133] == 6
+    assert r[139, 70, 70] == 63  # the bottom face is open: the medium continues
+
+
+def layered_small():
+    from ymc3d_b200.workloads import LAYER_ROWS, layered_vessel_geometry
+    return layered_vessel_geometry(64, 64, 32, 0.08), m.OpticalProps.from_tissues(LAYER_ROWS)
+
+
+@pytest.mark.parametrize("beam", ["uniform", "pencil"])
+def test_merged_vs_voxel_steps_chi2(table, beam):
+    g, p = layered_small()
+    mer = m.run([g], [p], [m.Job(0, 0, 2_000_000, 31, beam)], table=table)[0]
+    vox = m.run([g], [p], [m.Job(0, 0, 2_000_000, 32, beam)], table=table, steps="voxel")[0]
+    chi2, dof, pv = drs_chi2(mer.drs, mer.drs_sq, mer.photons, vox.drs, vox.drs_sq, vox.photons,
+                             f=4 if beam == "pencil" else 8)
+    assert dof > 20 and pv > 1e-4, (chi2, dof, pv)
+    for key in ("r_in", "r_out", "t_in", "absorbed"):
+        assert abs(total_z(mer.totals, vox.totals, key)) < 5, key
+    assert mer.totals["steps"] < vox.totals["steps"]
+
+
+def test_merged_steps_homogeneous_slab(table):
+    """a thick uniform slab, where nearly every flight is merged"""
+    g = m.Geometry(np.ones((60, 80, 80), np.uint8), 0.05, 0.05, 0.05)
+    p = m.OpticalProps.from_tissues([(0.02, 8.0, 0.9, 1.37)])
+    mer = m.run([g], [p], [m.Job(0, 0, 2_000_000, 41, "pencil")], table=table)[0]
+    vox = m.run([g], [p], [m.Job(0, 0, 2_000_000, 42, "pencil")], table=table,
+                steps="voxel")[0]
+    chi2, dof, pv = drs_chi2(mer.drs, mer.drs_sq, mer.photons, vox.drs, vox.drs_sq, vox.photons,
+                             f=2)
+    assert dof > 100 and pv > 1e-4, (chi2, dof, pv)
+    for key in ("r_in", "r_out", "t_in", "absorbed"):
+        assert abs(total_z(mer.totals, vox.totals, key)) < 5, key
+    assert mer.totals["steps"] * 2 < vox.totals["steps"]
+
+
+def test_merged_steps_conservation_and_absorption_map(table):
+    g, p = layered_small()
+    r = m.run([g], [p], [m.Job(0, 0, 500_000, 77, "uniform")], table=table,
+              absorption_map=True)[0]
+    t = r.totals
+    assert t["photons"] == 500_000 and residual(t) == 0
+    assert int(r.drs.sum()) == t["r_in"] and int(r.trans.sum()) == t["t_in"]
+    assert int(r.absorption.sum()) == t["absorbed"]
+
+
+def test_exact_math_ignores_step_mode(table):
+    g, p = layered_small()
+    job = m.Job(0, 0, 20_000, 9, "uniform")
+    a = m.run([g], [p], [job], table=table, math="exact")[0]
+    b = m.run([g], [p], [job], table=table, math="exact", steps="voxel")[0]
+    assert a.totals == b.totals and np.array_equal(a.drs, b.drs)
+
+
+
+def test_merged_steps_absorption_profile(table):
+    """the absorption map books each interaction in the voxel where it happens:
+    its depth profile agrees with per-face stepping"""
+    g, p = layered_small()
+    mer = m.run([g], [p], [m.Job(0, 0, 1_000_000, 51, "uniform")], table=table,
+                absorption_map=True)[0]
+    vox = m.run([g], [p], [m.Job(0, 0, 1_000_000, 52, "uniform")], table=table,
+                absorption_map=True, steps="voxel")[0]
+    a = mer.absorption.sum(axis=(1, 2)).astype(np.float64) / mer.totals["w_launched"]
+    b = vox.absorption.sum(axis=(1, 2)).astype(np.float64) / vox.totals["w_launched"]
+    big = b > 0.01 * b.max()
+    assert big.sum() > 5
+    assert np.max(np.abs(a[big] - b[big]) / b[big]) < 0.05

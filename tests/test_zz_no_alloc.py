@@ -27,7 +27,7 @@ def test_noalloc_matches_mc3d_run_twice(engine, table):
     p = engine.OpticalProps.from_tissues(LAYER_ROWS)
     tab = np.ascontiguousarray(table[:230401])  # MC3D_NOALLOC_MAX_TABLE lines
     job = engine.Job(0, 0, 300_000, 24681357, "uniform")
-    ref = engine.run([g], [p], [job], table=tab)[0]
+    ref = engine.run([g], [p], [job], table=tab, steps="voxel")[0]
 
     nx, ny, nz = g.shape
     dev = torch.device("cuda", 0)

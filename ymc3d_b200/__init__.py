@@ -32,6 +32,7 @@ STATUS_NAMES = {
 }
 BEAMS = {"uniform": 0, "pencil": 1}
 MATH = {"fast": 0, "exact": 1}
+STEPS = {"merged": 0, "voxel": 1}
 TOTAL_FIELDS = ("photons", "steps", "w_launched", "r_in", "r_out", "t_in", "t_out", "absorbed",
                 "rr_killed", "rr_created", "lost", "capped", "quickfix", "fresnel")
 DEFAULT_STREAMS = 1 << 40  # include/mc3d.h: one photon per stream unless a job says otherwise
@@ -79,7 +80,8 @@ class COptions(C.Structure):
     _fields_ = [("device", C.c_int32), ("math", C.c_int32), ("block", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("absorption_map", C.c_int32),
                 ("use_graph", C.c_int32), ("max_steps", C.c_int64),
-                ("photon_log", C.c_void_p), ("cancel", C.c_void_p)]
+                ("photon_log", C.c_void_p), ("cancel", C.c_void_p), ("steps", C.c_int32),
+                ("pad", C.c_int32)]
 
 
 class CRefGeometry(C.Structure):
@@ -114,6 +116,8 @@ EXPORTS = {
                                     C.c_void_p, C.c_void_p, C.c_int32]),
     "mc3d_mwc_draws": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                                  C.c_int32]),
+    "mc3d_safe_distance": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                     C.c_int32]),
     "mc3d_run_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                    C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p]),
@@ -263,11 +267,12 @@ class Result:
 
 
 def _options(device=0, math="fast", block=0, blocks_per_sm=0, max_steps=0, log=None,
-             cancel=None, absorption_map=False, use_graph=False) -> COptions:
+             cancel=None, absorption_map=False, use_graph=False, steps="merged") -> COptions:
     o = COptions()
     lib().mc3d_default_options(C.byref(o))
     o.device, o.math, o.block, o.blocks_per_sm, o.max_steps = (
         device, MATH[math], block, blocks_per_sm, max_steps)
+    o.steps = STEPS[steps]
     o.absorption_map = int(bool(absorption_map))
     o.use_graph = int(bool(use_graph))
     o.photon_log = _ptr(log)
@@ -312,11 +317,15 @@ def _finish(res, outs, jobs, log):
 def run(geoms: Sequence[Geometry], props: Sequence[OpticalProps], jobs: Sequence[Job],
         table: np.ndarray | None = None, math: str = "fast", device: int = 0, block: int = 0,
         blocks_per_sm: int = 0, max_steps: int = 0, photon_log: bool = False,
-        absorption_map: bool = False, cancel: np.ndarray | None = None) -> list[Result]:
+        absorption_map: bool = False, cancel: np.ndarray | None = None,
+        steps: str = "merged") -> list[Result]:
     """Run every job in one persistent launch (mc3d_run).  `cancel`, an int32 array
     of one element, is read by the kernel whenever a thread takes a new stream: set
     it non-zero (from another thread) to stop; the call then raises
-    MC3D_ERR_CANCELLED and the partial results are in the exception's .results."""
+    MC3D_ERR_CANCELLED and the partial results are in the exception's .results.
+    `steps` (fast math): "merged" joins the face crossings of a flight through
+    uniform tissue into one step, "voxel" steps at every voxel face like the
+    reference; exact math always steps per face."""
     table = default_table() if table is None else np.ascontiguousarray(table, dtype=np.uint32)
     g, p, j = _arrays(geoms, props, jobs)
     res, outs = _outs(geoms, jobs, absorption_map)
@@ -325,7 +334,7 @@ def run(geoms: Sequence[Geometry], props: Sequence[OpticalProps], jobs: Sequence
     if cancel is not None:
         cancel = np.ascontiguousarray(cancel, np.int32)
     opt = _options(device, math, block, blocks_per_sm, max_steps, log,
-                   absorption_map=absorption_map, cancel=cancel)
+                   absorption_map=absorption_map, cancel=cancel, steps=steps)
     st = lib().mc3d_run(g, len(geoms), p, len(props), j, len(jobs), table.ctypes.data,
                         len(table), C.byref(opt), outs)
     if st == -12:
@@ -340,11 +349,12 @@ class Plan:
     """Inputs resident on the device; execute() any number of times (mc3d_plan_*)."""
 
     def __init__(self, geoms, props, jobs, table=None, math="fast", device=0, block=0,
-                 blocks_per_sm=0, max_steps=0, use_graph=False):
+                 blocks_per_sm=0, max_steps=0, use_graph=False, steps="merged"):
         self.geoms, self.props, self.jobs = list(geoms), list(props), list(jobs)
         self.table = default_table() if table is None else np.ascontiguousarray(table, np.uint32)
         g, p, j = _arrays(self.geoms, self.props, self.jobs)
-        opt = _options(device, math, block, blocks_per_sm, max_steps, use_graph=use_graph)
+        opt = _options(device, math, block, blocks_per_sm, max_steps, use_graph=use_graph,
+                       steps=steps)
         self._h = C.c_void_p()
         _check(lib().mc3d_plan_create(C.byref(self._h), g, len(self.geoms), p, len(self.props),
                                       j, len(self.jobs), self.table.ctypes.data, len(self.table),
@@ -397,6 +407,22 @@ def mwc_draws(x: np.ndarray, a: np.ndarray, n: int, device: int = 0) -> np.ndarr
     out = np.zeros((len(x), n), np.float32)
     _check(lib().mc3d_mwc_draws(x.ctypes.data, a.ctypes.data, len(x), n, out.ctypes.data,
                                 device))
+    return out
+
+
+SAFE_CAP = 63
+
+
+def safe_distance(tissue: np.ndarray, device: int = 0) -> np.ndarray:
+    """The safe-distance map of MC3D_STEPS_MERGED for a [nz, ny, nx] uint8 grid,
+    [nz + 63, ny, nx]: per voxel the largest r <= 63 whose Chebyshev cube holds
+    only the voxel's tissue and stays below the top face and inside the lateral
+    faces; the medium continues below the grid with its last slice (computed on
+    the GPU)."""
+    t = np.ascontiguousarray(tissue, np.uint8)
+    nz, ny, nx = t.shape
+    out = np.zeros((nz + SAFE_CAP, ny, nx), np.uint8)
+    _check(lib().mc3d_safe_distance(t.ctypes.data, nx, ny, nz, out.ctypes.data, device))
     return out
 
 

@@ -17,7 +17,8 @@ from pathlib import Path
 
 from . import HERE, Job, Plan, default_table
 
-CANDIDATES = ((256, 0), (256, 4), (128, 0), (128, 8))
+# (threads per block, blocks per SM; 0 = as many as fit)
+CANDIDATES = ((256, 0), (128, 0), (64, 0))
 _CACHE_FILE = HERE / "_data" / "tuning.json"
 _cache: dict | None = None
 
@@ -42,7 +43,7 @@ def _save() -> None:
         pass
 
 
-def signature(geoms, props, jobs, math: str) -> str:
+def signature(geoms, props, jobs, math: str, steps: str = "merged") -> str:
     h = hashlib.sha1()
     for g in geoms:
         h.update(repr((g.shape, g.dx, g.dy, g.dz)).encode())
@@ -52,6 +53,7 @@ def signature(geoms, props, jobs, math: str) -> str:
     for j in jobs:
         h.update(repr((j.geom, j.props, j.beam, int(j.photons) // 1000)).encode())
     h.update(math.encode())
+    h.update(steps.encode())
     return h.hexdigest()[:16]
 
 
@@ -66,12 +68,12 @@ def _sample_jobs(jobs, streams_per_job: int):
 
 def tune(geoms, props, jobs, table=None, math: str = "fast", device: int = 0,
          candidates=CANDIDATES, sample_streams: int = 0, reps: int = 1,
-         use_cache: bool = True) -> dict:
+         use_cache: bool = True, steps: str = "merged") -> dict:
     """Return {"block", "blocks_per_sm", "ms", "table"} for the fastest candidate."""
     import torch
 
     dev_name = torch.cuda.get_device_name(device)
-    key = f"{dev_name}|{signature(geoms, props, jobs, math)}"
+    key = f"{dev_name}|{signature(geoms, props, jobs, math, steps)}"
     cache = _load()
     if use_cache and key in cache:
         return cache[key]
@@ -86,7 +88,7 @@ def tune(geoms, props, jobs, table=None, math: str = "fast", device: int = 0,
     for block, bps in candidates:
         try:
             plan = Plan(geoms, props, sample, table=table, math=math, device=device, block=block,
-                        blocks_per_sm=bps)
+                        blocks_per_sm=bps, steps=steps)
         except Exception:
             continue
         plan.execute(stream.cuda_stream)

@@ -31,6 +31,7 @@ UNITS = {
     "mc3d_kernel_exact.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
                              "-Xptxas", "-v"],
     "mc3d_seed.cu": ["-fmad=false"],
+    "mc3d_safedist.cu": [],
     "mc3d_api.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"],
     "mc3d_noalloc.cu": ["-use_fast_math", "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-v"],
 }

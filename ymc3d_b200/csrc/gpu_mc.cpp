@@ -7,6 +7,8 @@
  * (README.md:38), is read as an optional key=value file:
  *   photons=30000000  seed=<time>  beam=uniform|pencil  streams=0  math=fast|exact
  *   safeprimes=safeprimes_base32.txt  max_steps=0  device=0  abs_map=0  save_trans=0
+ *   steps=merged|voxel (fast math: merged crossings in uniform tissue, or one step
+ *   per voxel face like the reference)
  * An unreadable file (such as the README's "dummy_argument") keeps the defaults.
  * Differences: Total diffuse reflectance is the real total (the reference never
  * accumulates R_tot), and outname_report.json records the integer tallies.
@@ -33,6 +35,7 @@ struct Params {
     int beam = MC3D_BEAM_UNIFORM;
     long long streams = 0;
     int math = MC3D_MATH_FAST;
+    int steps = MC3D_STEPS_MERGED;
     std::string safeprimes = "safeprimes_base32.txt";
     long long max_steps = 0;
     int device = 0;
@@ -62,6 +65,7 @@ bool read_params(const char *path, Params &p)
         else if (k == "beam") p.beam = (v == "pencil") ? MC3D_BEAM_PENCIL : MC3D_BEAM_UNIFORM;
         else if (k == "streams") p.streams = std::stoll(v);
         else if (k == "math") p.math = (v == "exact") ? MC3D_MATH_EXACT : MC3D_MATH_FAST;
+        else if (k == "steps") p.steps = (v == "voxel") ? MC3D_STEPS_VOXEL : MC3D_STEPS_MERGED;
         else if (k == "safeprimes") p.safeprimes = v;
         else if (k == "max_steps") p.max_steps = std::stoll(v);
         else if (k == "device") p.device = std::stoi(v);
@@ -142,6 +146,7 @@ int main(int argc, char *argv[])
     mc3d_default_options(&opt);
     opt.device = prm.device;
     opt.math = prm.math;
+    opt.steps = prm.steps;
     opt.max_steps = prm.max_steps;
     opt.absorption_map = prm.abs_map ? 1 : 0;
 

@@ -132,7 +132,7 @@ int list_rejections_host(const mc3d_seed_consts &sc, uint64_t seed, const uint32
 struct mc3d_plan {
     int device = 0;
     int math = MC3D_MATH_FAST;
-    int variant = 0; /* fast kernel register budget, see launch_photon_fast */
+    int variant = 0; /* fast kernel variant bits (MC3D_VARIANT_*) */
     int block = 256;
     int grid = 0;
     size_t smem = 0;
@@ -143,6 +143,8 @@ struct mc3d_plan {
     int64_t total_bins = 0;
     int64_t total_photons = 0;
     std::vector<uint8_t *> d_grids;
+    std::vector<uint8_t *> d_radius; /* safe-distance maps (merged steps) */
+    bool jump = false;
     JobDev *d_jobs = nullptr;
     GeomDev *d_geoms = nullptr;
     float4 *d_props = nullptr;
@@ -171,6 +173,7 @@ static void plan_free(mc3d_plan *p)
     cudaSetDevice(p->device);
     if (p->stream) cudaStreamSynchronize(p->stream);
     for (uint8_t *g : p->d_grids) cudaFree(g);
+    for (uint8_t *r : p->d_radius) cudaFree(r);
     cudaFree(p->d_jobs);
     cudaFree(p->d_geoms);
     cudaFree(p->d_props);
@@ -216,6 +219,8 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     else mc3d_default_options(&opt);
     if (opt.math != MC3D_MATH_FAST && opt.math != MC3D_MATH_EXACT)
         return fail(MC3D_ERR_ARG, "unknown math mode %d", opt.math);
+    if (opt.steps != MC3D_STEPS_MERGED && opt.steps != MC3D_STEPS_VOXEL)
+        return fail(MC3D_ERR_ARG, "unknown step mode %d", opt.steps);
     if (opt.block < 0 || opt.block > 256 || (opt.block % 32) != 0)
         return fail(MC3D_ERR_ARG, "block must be a multiple of 32 up to 256, got %d", opt.block);
 
@@ -354,9 +359,12 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     /* ---- geometry grids and descriptors */
     std::vector<GeomDev> gh(ngeoms);
     p->d_grids.assign(ngeoms, nullptr);
+    p->jump = p->math == MC3D_MATH_FAST && opt.steps != MC3D_STEPS_VOXEL;
+    size_t max_map = 0; /* largest safe-distance map, nz + MC3D_SAFE_CAP slices */
     for (int i = 0; i < ngeoms; i++) {
         const mc3d_geom &g = geoms[i];
         size_t nv = (size_t)g.nx * g.ny * g.nz;
+        max_map = std::max(max_map, (size_t)g.nx * g.ny * (g.nz + MC3D_SAFE_CAP));
         PLAN_TRY(cudaMalloc(&p->d_grids[i], nv));
         PLAN_TRY(cudaMemcpyAsync(p->d_grids[i], g.tissue, nv, cudaMemcpyHostToDevice, p->stream));
         GeomDev &d = gh[i];
@@ -367,6 +375,23 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         d.Lx = d.dx * g.nx; d.Ly = d.dy * g.ny; d.Lz = d.dz * g.nz;
         d.rdx = 1.0f / d.dx; d.rdy = 1.0f / d.dy; d.rdz = 1.0f / d.dz;
         d.tissue = p->d_grids[i];
+    }
+    if (p->jump) {
+        p->d_radius.assign(ngeoms, nullptr);
+        uint8_t *tmp = nullptr;
+        PLAN_TRY(cudaMalloc(&tmp, 2 * max_map));
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < ngeoms && e == cudaSuccess; i++) {
+            size_t nmap = (size_t)geoms[i].nx * geoms[i].ny * (geoms[i].nz + MC3D_SAFE_CAP);
+            e = cudaMalloc(&p->d_radius[i], nmap);
+            if (e == cudaSuccess)
+                e = launch_safe_distance(p->d_grids[i], geoms[i].nx, geoms[i].ny, geoms[i].nz,
+                                         p->d_radius[i], tmp, tmp + max_map, p->stream);
+            gh[i].radius = p->d_radius[i];
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+        cudaFree(tmp);
+        PLAN_TRY(e);
     }
     PLAN_TRY(cudaMalloc(&p->d_geoms, sizeof(GeomDev) * ngeoms));
     PLAN_TRY(cudaMemcpyAsync(p->d_geoms, gh.data(), sizeof(GeomDev) * ngeoms,
@@ -452,13 +477,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         PLAN_TRY(p->math == MC3D_MATH_FAST ? smem_limit_photon_fast(p->smem)
                                           : smem_limit_photon_exact(p->smem));
     }
-    /* four or more blocks of 256 per SM need the 64-register variant */
-    p->variant = (p->math == MC3D_MATH_FAST && !opt.absorption_map &&
-                  (int64_t)opt.blocks_per_sm * p->block >= 1024) ? 1 : 0;
-    /* experiment knob: the fast kernel on the split step (photon_step_fast) */
-    const char *fs = getenv("MC3D_FAST_STEP");
-    if (p->math == MC3D_MATH_FAST && !opt.absorption_map && fs && !strcmp(fs, "split"))
-        p->variant = 2;
+    p->variant = p->jump ? 0 : MC3D_VARIANT_VOXEL_STEPS;
     int bps = 0;
     PLAN_TRY(p->math == MC3D_MATH_FAST ? occupancy_photon_fast(p->block, p->smem, &bps, p->variant)
                                       : occupancy_photon_exact(p->block, p->smem, &bps));
@@ -695,6 +714,25 @@ int mc3d_mwc_draws(const uint64_t *x, const uint32_t *a, int64_t ngen, int64_t n
     cudaFree(d_a);
     cudaFree(d_o);
     if (e != cudaSuccess) return fail(MC3D_ERR_CUDA, "mwc draws: %s", cudaGetErrorString(e));
+    return MC3D_OK;
+}
+
+int mc3d_safe_distance(const uint8_t *tissue, int32_t nx, int32_t ny, int32_t nz,
+                       uint8_t *radius, int32_t device)
+{
+    if (!tissue || !radius || nx <= 0 || ny <= 0 || nz <= 0)
+        return fail(MC3D_ERR_ARG, "bad arguments");
+    CUDA_TRY(cudaSetDevice(device));
+    const size_t nv = (size_t)nx * ny * nz;
+    const size_t nm = (size_t)nx * ny * (nz + MC3D_SAFE_CAP);
+    uint8_t *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, nv + 3 * nm); /* grid | map | two scratch maps */
+    if (e == cudaSuccess) e = cudaMemcpy(d, tissue, nv, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = launch_safe_distance(d, nx, ny, nz, d + nv, d + nv + nm, d + nv + 2 * nm, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(radius, d + nv, nm, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(MC3D_ERR_CUDA, "safe distance: %s", cudaGetErrorString(e));
     return MC3D_OK;
 }
 

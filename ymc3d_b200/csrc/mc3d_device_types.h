@@ -14,6 +14,10 @@
 /* order of the per-job totals (matches mc3d_totals in include/mc3d.h) */
 #define MC3D_NUM_TOTALS 14
 
+/* largest safe distance of the merged-step map, and the number of slices the
+ * map adds below the grid (the clamped continuation of the medium) */
+#define MC3D_SAFE_CAP 63
+
 namespace mc3d {
 
 struct GeomDev {
@@ -23,6 +27,7 @@ struct GeomDev {
     float rdx, rdy, rdz;   /* 1 / voxel size (fast math only) */
     float pad2;
     const uint8_t *tissue; /* nz*ny*nx, x fastest; 0 = air */
+    const uint8_t *radius; /* safe-distance map, nz + MC3D_SAFE_CAP slices (merged steps) */
 };
 
 struct JobDev {

@@ -87,6 +87,8 @@ struct MathFast {
 #define MC3D_W_THRESHOLD_LE_F 0x1.a36e2ep-14f
 #define MC3D_UZ_THRESH 0.99999
 #define MC3D_UZ_THRESH_LE_F 0x1.fffeb0p-1f
+/* fast math: |1 - sin^2(theta_t)| below this takes the FP64 Fresnel branch */
+#define MC3D_NEAR_CRITICAL_F 0x1p-5f
 #define MC3D_NUM_PHOTON_STEPS 45
 #define MC3D_TISSUE_AIR 0
 #define MC3D_TAB_STRIDE 3 /* float4 per tissue in the optical table */
@@ -108,33 +110,45 @@ static __device__ __forceinline__ int grid_coord(float x, float ux, float d, flo
     return i;
 }
 
-/* src/mc3d_gpu.cu:24-27 with the clamp addressing of the texture (:416-418) */
+/* src/mc3d_gpu.cu:24-27 with the clamp addressing of the texture (:416-418).
+ * With JUMP the voxel's safe distance rides in bits 8-15 of the result (0 above
+ * the surface, where the tissue is air). */
+template <bool JUMP = false>
 static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, int k, float z,
                                                 float uz)
 {
     int ci = min(max(i, 0), g.nx - 1);
     int cj = min(max(j, 0), g.ny - 1);
     int ck = min(max(k, 0), g.nz - 1);
-    int t = __ldg(g.tissue + ((int64_t)ck * g.ny + cj) * g.nx + ci);
+    const int64_t col = (int64_t)cj * g.nx + ci;
+    int t = __ldg(g.tissue + (int64_t)ck * g.ny * g.nx + col);
+    if (JUMP) {
+        const int rk = min(max(k, 0), g.nz - 1 + MC3D_SAFE_CAP);
+        t |= (int)__ldg(g.radius + (int64_t)rk * g.ny * g.nx + col) << 8;
+    }
     return ((z <= 0) && (uz < 0)) ? MC3D_TISSUE_AIR : t;
 }
 
-/* src/mc3d_gpu.cu:29-49 */
+/* src/mc3d_gpu.cu:29-49.  With r > 0 the box is the cube of voxels within
+ * Chebyshev distance r of (i, j, k) instead of the voxel itself; axes, if given,
+ * receives the snapped axes (bit 0 x, 1 y, 2 z). */
 template <class M>
 static __device__ __forceinline__ float intersection(const GeomDev &g, int i, int j, int k,
                                                      float *x, float ux, float *y, float uy,
-                                                     float *z, float uz)
+                                                     float *z, float uz, int r = 0,
+                                                     int *axes = nullptr)
 {
-    float border_x = (float)((ux >= 0) ? (int)((unsigned)i + 1u) : i) * g.dx;
+    float border_x = (float)((ux >= 0) ? (int)((unsigned)i + 1u + r) : i - r) * g.dx;
     float t_x = M::div(border_x - *x, ux);
-    float border_y = (float)((uy >= 0) ? (int)((unsigned)j + 1u) : j) * g.dy;
+    float border_y = (float)((uy >= 0) ? (int)((unsigned)j + 1u + r) : j - r) * g.dy;
     float t_y = M::div(border_y - *y, uy);
-    float border_z = (float)((uz >= 0) ? (int)((unsigned)k + 1u) : k) * g.dz;
+    float border_z = (float)((uz >= 0) ? (int)((unsigned)k + 1u + r) : k - r) * g.dz;
     float t_z = M::div(border_z - *z, uz);
     float t = fminf(t_x, fminf(t_y, t_z));
     *x = (t == t_x) ? border_x : *x + ux * t;
     *y = (t == t_y) ? border_y : *y + uy * t;
     *z = (t == t_z) ? border_z : *z + uz * t;
+    if (axes) *axes = (int)(t == t_x) | ((int)(t == t_y) << 1) | ((int)(t == t_z) << 2);
     return t;
 }
 
@@ -172,8 +186,17 @@ struct Acc {
 };
 
 /* One step of src/mc3d_gpu.cu:175-340 for a live photon.  Returns true when the
- * photon froze during this step; *db receives the step's boundary distance. */
-template <class M, bool AMAP>
+ * photon froze during this step; *db receives the step's boundary distance.
+ *
+ * JUMP (merged steps): p.tissue carries the voxel's safe distance r in bits 8-15,
+ * and the step's box is the cube of voxels within Chebyshev distance r of the
+ * photon's voxel, all of the photon's tissue.  Its faces are voxel faces, so a
+ * step that reaches one ends exactly where the reference's step at that face
+ * ends (snapped, next voxel by the face rule, Fresnel, mirror), while the face
+ * crossings inside the cube, which in the reference only move the photon (no
+ * Fresnel event, absorption or scattering; their four random numbers are drawn
+ * and discarded), are merged into this one step. */
+template <class M, bool AMAP, bool JUMP = false>
 static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float4 *tab,
                                                    Photon &p, uint64_t &rx, uint32_t ra,
                                                    const Acc &acc, float *db_out,
@@ -182,9 +205,10 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
 {
     /* per tissue: (mua, mus, g, n), (mu_t, mua/mu_t, 1/mu_t, 1/(2g)),
      * (1-g^2, 1-g, 2g, 1+g^2) -- each the float the reference computes per step */
-    const float4 t0 = tab[MC3D_TAB_STRIDE * p.tissue];
-    const float4 t1 = tab[MC3D_TAB_STRIDE * p.tissue + 1];
-    const float4 t2 = tab[MC3D_TAB_STRIDE * p.tissue + 2];
+    const int tis = JUMP ? (p.tissue & 0xff) : p.tissue;
+    const float4 t0 = tab[MC3D_TAB_STRIDE * tis];
+    const float4 t1 = tab[MC3D_TAB_STRIDE * tis + 1];
+    const float4 t2 = tab[MC3D_TAB_STRIDE * tis + 2];
     float ni = t0.w;
     float nt = ni;
     float mu_a = t0.x;
@@ -192,7 +216,9 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     (void)mu_a;
 
     float newx = p.x, newy = p.y, newz = p.z;
-    float db = intersection<M>(g, p.i, p.j, p.k, &newx, p.ux, &newy, p.uy, &newz, p.uz);
+    int axes = 0;
+    float db = intersection<M>(g, p.i, p.j, p.k, &newx, p.ux, &newy, p.uy, &newz, p.uz,
+                               JUMP ? (p.tissue >> 8) : 0, JUMP ? &axes : nullptr);
 
     bool hit = db * mu_t <= p.s;
     float ds = hit ? db * mu_t : p.s;
@@ -204,13 +230,24 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     int nexti = grid_coord<M>(newx, p.ux, g.dx, g.rdx);
     int nextj = grid_coord<M>(newy, p.uy, g.dy, g.rdy);
     int nextk = grid_coord<M>(newz, p.uz, g.dz, g.rdz);
-    int next_tissue = tissue_at(g, nexti, nextj, nextk, newz, p.uz);
-    nt = tab[MC3D_TAB_STRIDE * next_tissue].w;
+    int next_tissue = tissue_at<JUMP>(g, nexti, nextj, nextk, newz, p.uz);
+    nt = tab[MC3D_TAB_STRIDE * (JUMP ? (next_tissue & 0xff) : next_tissue)].w;
+
+    /* The voxel on the near side of the crossed face, which the reference's face
+     * logic compares with the next voxel: the photon's own voxel in a one-voxel
+     * step, the last voxel of the cube in a merged one. */
+    int bi = p.i, bj = p.j, bk = p.k;
+    if (JUMP) {
+        const int ax = hit ? axes : 0;
+        bi = nexti - ((ax & 1) ? ((p.ux >= 0) ? 1 : -1) : 0);
+        bj = nextj - ((ax & 2) ? ((p.uy >= 0) ? 1 : -1) : 0);
+        bk = nextk - ((ax & 4) ? ((p.uz >= 0) ? 1 : -1) : 0);
+    }
 
     float tr_ux = p.ux, tr_uy = p.uy, tr_uz = p.uz;
     bool refl = false;
     if (ni != nt) { /* src/mc3d_gpu.cu:226-257 */
-        float cos_ai = (p.i != nexti) ? p.ux : ((p.j != nextj) ? p.uy : p.uz);
+        float cos_ai = (bi != nexti) ? p.ux : ((bj != nextj) ? p.uy : p.uz);
         cos_ai = fabsf(cos_ai);
         cos_ai = (cos_ai > 1) ? 1 : cos_ai;
         float ai = M::acos(cos_ai);
@@ -223,17 +260,41 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
         float R = 0.5 * R1 * R1 * (1.0f + R2 * R2);
         R = (sin_at > 1) ? 1 : R;
         R = (ni == nt) ? 0 : R;
+        float lat = ni_nt; /* scale of the transmitted lateral cosines */
+        if (M::kFast && fabsf(1.0f - sin_at * sin_at) < MC3D_NEAR_CRITICAL_F) {
+            /* Near the critical angle 1 - sin_at^2 cancels in float and R is steep:
+             * the same formulas in FP64, sin_ai from cos_ai directly, and the
+             * transmitted direction renormalised in FP64. */
+            const double c = cos_ai;
+            const double rn = (double)ni / (double)nt;
+            const double si = sqrt((1.0 - c) * (1.0 + c));
+            const double st = rn * si;
+            const double ca = sqrt(fmax((1.0 - st) * (1.0 + st), 0.0));
+            const double R1 = (si * ca - c * st) / (si * ca + c * st);
+            const double R2 = (c * ca - si * st) / (c * ca + st * st);
+            R = (st >= 1.0) ? 1.0f : (float)(0.5 * R1 * R1 * (1.0 + R2 * R2));
+            const bool xa = bi != nexti;
+            const bool ya = !xa && bj != nextj;
+            const bool za = !xa && !ya && bk != nextk;
+            const double ax = xa ? 0.0 : (double)p.ux;
+            const double ay = ya ? 0.0 : (double)p.uy;
+            const double az = za ? 0.0 : (double)p.uz;
+            const double lat2 = rn * rn * (ax * ax + ay * ay + az * az);
+            const double sc = 1.0 / sqrt(ca * ca + lat2);
+            cos_at = (float)(ca * sc);
+            lat = (float)(rn * sc);
+        }
         float eps = mc3d_rand_co(&rx, ra);
         refl = eps < R;
-        tr_ux = refl ? p.ux * ((p.i == nexti) ? 1 : -1)
-                     : ((p.i != nexti) ? copysignf(cos_at, p.ux * cos_at) : p.ux * ni_nt);
-        tr_uy = refl ? p.uy * ((p.j == nextj) ? 1 : -1)
-                     : (((p.j != nextj) && (p.i == nexti)) ? copysignf(cos_at, p.uy * cos_at)
-                                                           : p.uy * ni_nt);
-        tr_uz = refl ? p.uz * ((p.k == nextk) ? 1 : -1)
-                     : (((p.k != nextk) && (p.j == nextj) && (p.i == nexti))
+        tr_ux = refl ? p.ux * ((bi == nexti) ? 1 : -1)
+                     : ((bi != nexti) ? copysignf(cos_at, p.ux * cos_at) : p.ux * lat);
+        tr_uy = refl ? p.uy * ((bj == nextj) ? 1 : -1)
+                     : (((bj != nextj) && (bi == nexti)) ? copysignf(cos_at, p.uy * cos_at)
+                                                           : p.uy * lat);
+        tr_uz = refl ? p.uz * ((bk == nextk) ? 1 : -1)
+                     : (((bk != nextk) && (bj == nextj) && (bi == nexti))
                             ? copysignf(cos_at, p.uz * cos_at)
-                            : p.uz * ni_nt);
+                            : p.uz * lat);
         (*fresnel_count)++;
     }
 
@@ -244,10 +305,12 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     W = W - dW * (float)(!hit);
     if (AMAP && !hit && mu_t > 0) {
         /* absorption map, the reference's disabled tally (src/mc3d_gpu.cu:265-272):
-         * the current voxel clamped into the grid, fixed-point weight removed */
-        int ai = min(max(p.i, 0), g.nx - 1);
-        int aj = min(max(p.j, 0), g.ny - 1);
-        int ak = min(max(p.k, 0), g.nz - 1);
+         * the current voxel clamped into the grid, fixed-point weight removed.  A
+         * merged step can end its flight several voxels from where it started, so
+         * there the voxel of the interaction point is used. */
+        int ai = min(max(JUMP ? nexti : p.i, 0), g.nx - 1);
+        int aj = min(max(JUMP ? nextj : p.j, 0), g.ny - 1);
+        int ak = min(max(JUMP ? nextk : p.k, 0), g.nz - 1);
         uint64_t dq = qw(W_before) - qw(W);
         if (dq) atomicAdd(amap + ((int64_t)ak * g.ny + aj) * g.nx + ai, (unsigned long long)dq);
     }
@@ -323,192 +386,20 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     *lat_mirror = refl && !fres_refl;
 
     bool keep = (hit && refl) || freeze;
-    p.i = keep ? p.i : nexti;
-    p.j = keep ? p.j : nextj;
-    p.k = keep ? p.k : nextk;
-    p.tissue = keep ? p.tissue : next_tissue;
-    *db_out = db;
-    return freeze;
-}
-
-/* ------------------------------------------------------------ fast-math step
- * The same physics as photon_step, organised for SIMT throughput:
- *  - a face crossing only snaps, moves and looks up the next voxel.  The four
- *    random numbers the reference draws on a crossing (roulette, two for the
- *    Henyey-Greenstein spin, a new path length) are all discarded there, so
- *    they are not drawn: the photon's statistics are unchanged while the random
- *    stream is consumed only by the draws that decide something;
- *  - cell indices move by one on the snapped axes; the other axes are kept when
- *    the new position lies strictly inside the cell, and otherwise recomputed
- *    with photontrack_get_grid_coord's rule;
- *  - absorption, roulette, scattering and the new path length run only for the
- *    lanes whose step ends in the tissue, behind one branch;
- *  - a crossing without a Fresnel event keeps its direction unnormalised again.
- * Returns true when the photon froze; *db receives the boundary distance. */
-template <bool AMAP>
-static __device__ __forceinline__ bool photon_step_fast(const GeomDev &g, const float4 *tab,
-                                                        Photon &p, uint64_t &rx, uint32_t ra,
-                                                        const Acc &acc, float *db_out,
-                                                        uint32_t *fresnel_count,
-                                                        unsigned long long *amap,
-                                                        bool *lat_mirror)
-{
-    typedef MathFast M;
-    const float4 t0 = tab[MC3D_TAB_STRIDE * p.tissue];
-    const float4 t1 = tab[MC3D_TAB_STRIDE * p.tissue + 1];
-    const float ni = t0.w;
-    const float mu_t = t1.x;
-
-    /* DDA to the next face, src/mc3d_gpu.cu:29-49 */
-    const int si = (p.ux >= 0) ? 1 : 0, sj = (p.uy >= 0) ? 1 : 0, sk = (p.uz >= 0) ? 1 : 0;
-    const float bx = (float)(p.i + si) * g.dx;
-    const float by = (float)(p.j + sj) * g.dy;
-    const float bz = (float)(p.k + sk) * g.dz;
-    const float tx = __fdividef(bx - p.x, p.ux);
-    const float ty = __fdividef(by - p.y, p.uy);
-    const float tz = __fdividef(bz - p.z, p.uz);
-    const float db = fminf(tx, fminf(ty, tz));
-    const bool hit = db * mu_t <= p.s;
-    const bool hx = hit && (db == tx), hy = hit && (db == ty), hz = hit && (db == tz);
-
-    /* new position: the face (snapped) or the interaction point s / mu_t away */
-    const float dist = hit ? db : p.s * t1.z;
-    float newx = hx ? bx : p.x + p.ux * dist;
-    float newy = hy ? by : p.y + p.uy * dist;
-    float newz = hz ? bz : p.z + p.uz * dist;
-    const float s_left = hit ? p.s - db * mu_t : 0.0f;
-
-    /* next cell: +-1 on a snapped axis, unchanged where strictly inside */
-    int nexti = hx ? p.i + 2 * si - 1 : p.i;
-    int nextj = hy ? p.j + 2 * sj - 1 : p.j;
-    int nextk = hz ? p.k + 2 * sk - 1 : p.k;
-    /* the cell's other face on each axis (the DDA border is the first) */
-    const float ox = (float)(p.i + 1 - si) * g.dx;
-    const float oy = (float)(p.j + 1 - sj) * g.dy;
-    const float oz = (float)(p.k + 1 - sk) * g.dz;
-    const bool okx = hx || (newx > fminf(bx, ox) && newx < fmaxf(bx, ox));
-    const bool oky = hy || (newy > fminf(by, oy) && newy < fmaxf(by, oy));
-    const bool okz = hz || (newz > fminf(bz, oz) && newz < fmaxf(bz, oz));
-    if (!(okx && oky && okz)) {
-        nexti = grid_coord<M>(newx, p.ux, g.dx, g.rdx);
-        nextj = grid_coord<M>(newy, p.uy, g.dy, g.rdy);
-        nextk = grid_coord<M>(newz, p.uz, g.dz, g.rdz);
-    }
-    int next_tissue = p.tissue;
-    if (nexti != p.i || nextj != p.j || nextk != p.k || newz <= 0)
-        next_tissue = tissue_at(g, nexti, nextj, nextk, newz, p.uz);
-
-    float W = p.W;
-    float nux = p.ux, nuy = p.uy, nuz = p.uz;
-    bool refl = false, renorm = false;
-    bool freeze = (mu_t == 0);
-    float s_new = s_left;
-    if (hit) {
-        const float nt = tab[MC3D_TAB_STRIDE * next_tissue].w;
-        if (ni != nt) { /* Fresnel, src/mc3d_gpu.cu:226-257 */
-            float cos_ai = (p.i != nexti) ? p.ux : ((p.j != nextj) ? p.uy : p.uz);
-            cos_ai = fabsf(cos_ai);
-            cos_ai = (cos_ai > 1) ? 1 : cos_ai;
-            float ai = acosf(cos_ai);
-            float ni_nt = M::div(ni, nt);
-            float sin_ai = sinf(ai);
-            float sin_at = ni_nt * sin_ai;
-            float cos_at = sqrtf(1.0f - sin_at * sin_at);
-            float R1 = M::div(sin_ai * cos_at - cos_ai * sin_at, sin_ai * cos_at + cos_ai * sin_at);
-            float R2 = M::div(cos_ai * cos_at - sin_ai * sin_at, cos_ai * cos_at + sin_at * sin_at);
-            float R = 0.5 * R1 * R1 * (1.0f + R2 * R2);
-            R = (sin_at > 1) ? 1 : R;
-            float eps = mc3d_rand_co(&rx, ra);
-            refl = eps < R;
-            nux = refl ? p.ux * ((p.i == nexti) ? 1 : -1)
-                       : ((p.i != nexti) ? copysignf(cos_at, p.ux * cos_at) : p.ux * ni_nt);
-            nuy = refl ? p.uy * ((p.j == nextj) ? 1 : -1)
-                       : (((p.j != nextj) && (p.i == nexti)) ? copysignf(cos_at, p.uy * cos_at)
-                                                             : p.uy * ni_nt);
-            nuz = refl ? p.uz * ((p.k == nextk) ? 1 : -1)
-                       : (((p.k != nextk) && (p.j == nextj) && (p.i == nexti))
-                              ? copysignf(cos_at, p.uz * cos_at)
-                              : p.uz * ni_nt);
-            renorm = true;
-            (*fresnel_count)++;
-        }
+    if (JUMP) {
+        /* a reflected photon stays on the near side of the face: that voxel has
+         * the photon's tissue; its safe distance is not at hand, so 0 (one
+         * per-face step) until the photon moves on */
+        const bool back = hit && refl && !freeze;
+        p.i = freeze ? p.i : (back ? bi : nexti);
+        p.j = freeze ? p.j : (back ? bj : nextj);
+        p.k = freeze ? p.k : (back ? bk : nextk);
+        p.tissue = freeze ? p.tissue : (back ? (p.tissue & 0xff) : next_tissue);
     } else {
-        /* absorption, src/mc3d_gpu.cu:262-263 */
-        const float W_before = W;
-        if (mu_t > 0) W = W - t1.y * W;
-        if (AMAP && mu_t > 0) {
-            int ai = min(max(p.i, 0), g.nx - 1);
-            int aj = min(max(p.j, 0), g.ny - 1);
-            int ak = min(max(p.k, 0), g.nz - 1);
-            uint64_t dq = qw(W_before) - qw(W);
-            if (dq) atomicAdd(amap + ((int64_t)ak * g.ny + aj) * g.nx + ai, (unsigned long long)dq);
-        }
-        /* russian roulette, src/mc3d_gpu.cu:275-277 */
-        float eps = mc3d_rand_co(&rx, ra);
-        if ((W <= MC3D_W_THRESHOLD_LE_F) && (mu_t != 0)) {
-            float newW = (eps < MC3D_SURVIVAL_LT_F) ? (float)((double)W / MC3D_SURVIVAL_CHANCE)
-                                                     : 0.0f;
-            if (newW == 0.0f) {
-                uint64_t k = qw(W);
-                acc[T_RR_KILLED] += k;
-                acc[T_ABSORBED] -= k;
-            } else {
-                uint64_t c = qw(newW) - qw(W);
-                acc[T_RR_CREATED] += c;
-                acc[T_ABSORBED] += c;
-            }
-            W = newW;
-        }
-        /* Henyey-Greenstein, src/mc3d_gpu.cu:282-294 */
-        const float4 t2 = tab[MC3D_TAB_STRIDE * p.tissue + 2];
-        float costheta = M::div(t2.x, t2.y + t2.z * mc3d_rand_oc(&rx, ra));
-        costheta = t1.w * (t2.w - costheta * costheta);
-        float sintheta = sqrtf(1 - costheta * costheta);
-        float cosphi, sinphi;
-        M::sincospi(2 * mc3d_rand_co(&rx, ra), &sinphi, &cosphi);
-        const float one_uz2 = 1 - p.uz * p.uz;
-        const float invsqrt = rsqrtf(one_uz2);
-        const bool steep = !(fabsf(p.uz) <= MC3D_UZ_THRESH_LE_F);
-        nux = !steep ? sintheta * (p.ux * p.uz * cosphi - p.uy * sinphi) * invsqrt +
-                           p.ux * costheta
-                     : sintheta * cosphi;
-        nuy = !steep ? sintheta * (p.uy * p.uz * cosphi + p.ux * sinphi) * invsqrt +
-                           p.uy * costheta
-                     : sintheta * sinphi;
-        nuz = !steep ? -one_uz2 * invsqrt * sintheta * cosphi + p.uz * costheta
-                     : copysignf(costheta, costheta * p.uz);
-        renorm = true;
-        freeze = freeze || (W <= 0);
-        /* new path length, src/mc3d_gpu.cu:319-321 */
-        const float e2 = mc3d_rand_oc(&rx, ra);
-        s_new = (W > 0) ? -__logf(e2) : 0;
-    }
-    if (renorm) {
-        const float zero_thresh = (float)(1 - MC3D_UZ_THRESH);
-        nux = (fabsf(nux) < zero_thresh) ? 0 : nux;
-        nuy = (fabsf(nuy) < zero_thresh) ? 0 : nuy;
-        nuz = (fabsf(nuz) < zero_thresh) ? 0 : nuz;
-        float norm = rsqrtf(nux * nux + nuy * nuy + nuz * nuz);
-        nux *= norm;
-        nuy *= norm;
-        nuz *= norm;
-    }
-    p.W = W;
-    if (!freeze) {
-        p.ux = nux; p.uy = nuy; p.uz = nuz;
-        p.x = newx; p.y = newy; p.z = newz;
-        p.s = s_new;
-    } else {
-        p.s = s_left;
-    }
-    /* mirror, short-circuited by a Fresnel reflection (src/mc3d_gpu.cu:330) */
-    const bool fres_refl = refl;
-    if (!(p.x > 0 && p.x < g.Lx && p.y > 0 && p.y < g.Ly))
-        refl = refl || mirror(&p.x, &p.ux, g.Lx) || mirror(&p.y, &p.uy, g.Ly);
-    *lat_mirror = refl && !fres_refl;
-    if (!((hit && refl) || freeze)) {
-        p.i = nexti; p.j = nextj; p.k = nextk;
-        p.tissue = next_tissue;
+        p.i = keep ? p.i : nexti;
+        p.j = keep ? p.j : nextj;
+        p.k = keep ? p.k : nextk;
+        p.tissue = keep ? p.tissue : next_tissue;
     }
     *db_out = db;
     return freeze;
@@ -516,13 +407,13 @@ static __device__ __forceinline__ bool photon_step_fast(const GeomDev &g, const 
 
 /* i, j, k and tissue from the position, as at the start of every launch of
  * photontrack_step (src/mc3d_gpu.cu:168-171). */
-template <class M>
+template <class M, bool JUMP = false>
 static __device__ __forceinline__ void derive_cell(const GeomDev &g, Photon &p)
 {
     p.i = grid_coord<M>(p.x, p.ux, g.dx, g.rdx);
     p.j = grid_coord<M>(p.y, p.uy, g.dy, g.rdy);
     p.k = grid_coord<M>(p.z, p.uz, g.dz, g.rdz);
-    p.tissue = tissue_at(g, p.i, p.j, p.k, p.z, p.uz);
+    p.tissue = tissue_at<JUMP>(g, p.i, p.j, p.k, p.z, p.uz);
 }
 
 /* Whether photontrack_get_grid_coord's face rule puts (x, u) in the stored cell on
@@ -623,10 +514,9 @@ static __device__ __forceinline__ uint64_t stream_seed(const KernelParams &P, co
     return mc3d_seed_attempt(xs, P.seed.begin, fora);
 }
 
-/* SPLIT selects photon_step_fast for the fast policy; the default runs the
- * reference-structured photon_step with fast math, which measured 11-15 % faster
- * (its branch-free selects keep warps converged better than the split's branches) */
-template <class M, bool AMAP, bool SPLIT = false>
+/* The persistent photon loop.  JUMP selects merged steps (photon_step) and needs
+ * every geometry's safe-distance map. */
+template <class M, bool AMAP, bool JUMP = false>
 __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
 {
     extern __shared__ float4 sh_tab[];
@@ -686,7 +576,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
             p.W = 1.0f - rsp;
             qw0 = qw(p.W);
             p.s = -M::log(mc3d_rand_oc(&rx, ra));
-            derive_cell<M>(g, p);
+            derive_cell<M, JUMP>(g, p);
             chunk = 0;
             psteps = 0;
             fresnel = 0;
@@ -697,12 +587,8 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
         float db;
         bool lat_mirror;
         bool froze;
-        if constexpr (M::kFast && SPLIT)
-            froze = photon_step_fast<AMAP>(g, tab, p, rx, ra, acc, &db, &fresnel, amap,
+        froze = photon_step<M, AMAP, JUMP>(g, tab, p, rx, ra, acc, &db, &fresnel, amap,
                                            &lat_mirror);
-        else
-            froze = photon_step<M, AMAP>(g, tab, p, rx, ra, acc, &db, &fresnel, amap,
-                                         &lat_mirror);
         chunk++;
         psteps++;
 
@@ -726,7 +612,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
             } else {
                 /* fast math: re-derive only where the stored cell breaks the face rule
                  * (exact math always re-derives, as the reference's relaunch does) */
-                if (!M::kFast || !cell_consistent(g, p)) derive_cell<M>(g, p);
+                if (!M::kFast || !cell_consistent(g, p)) derive_cell<M, JUMP>(g, p);
                 chunk = 0;
             }
         }
@@ -771,7 +657,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
                 r.ux = p.ux; r.uy = p.uy; r.uz = p.uz;
                 r.W = p.W; r.s = p.s;
                 r.steps = psteps;
-                r.tissue = (uint32_t)p.tissue;
+                r.tissue = (uint32_t)(p.tissue & 0xff);
                 r.rng = rx;
                 P.photon_log[pid] = r;
             }

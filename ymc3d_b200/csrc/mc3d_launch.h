@@ -11,8 +11,11 @@
 
 namespace mc3d {
 
-/* variant 0: 80-register budget (3 blocks of 256 per SM); 1: 64 registers (4 blocks);
- * 2: the split step photon_step_fast (A/B experiments) */
+/* fast kernel variant bits: one step per voxel face instead of merged steps.
+ * (A 64-register build of 4 blocks of 256 per SM measured 2-12 % slower than the
+ * 80-register one and is not built: one kernel serves every launch shape, so the
+ * tallies cannot depend on the shape.) */
+#define MC3D_VARIANT_VOXEL_STEPS 2
 cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_t smem,
                                cudaStream_t stream, int variant);
 cudaError_t launch_photon_exact(const KernelParams &P, int grid, int block, size_t smem,
@@ -31,6 +34,10 @@ cudaError_t launch_seed_scan(const JobDev *jobs, int njobs, const uint32_t *mult
 /* states of streams [first, first+count) of job 0 of `jobs` */
 cudaError_t launch_seed_dump(const KernelParams &P, int64_t first, int64_t count,
                              uint64_t *x_out, uint32_t *a_out, cudaStream_t stream);
+/* safe-distance map of a tissue grid (merged steps): out, tmp_a and tmp_b hold
+ * nx * ny * (nz + MC3D_SAFE_CAP) bytes each */
+cudaError_t launch_safe_distance(const uint8_t *tissue, int nx, int ny, int nz, uint8_t *out,
+                                 uint8_t *tmp_a, uint8_t *tmp_b, cudaStream_t stream);
 cudaError_t launch_mwc_draws(const uint64_t *x, const uint32_t *a, int64_t ngen, int64_t n,
                              float *out, cudaStream_t stream);
 
