@@ -88,6 +88,22 @@ def test_batched_equals_separate(table):
         assert np.array_equal(r.drs, alone.drs)
 
 
+def test_many_geometries_batched_equals_separate(table):
+    """64 geometries in one launch (descriptors and tables in shared memory,
+    with the tally columns over 48 KB per block): each job's tallies equal its
+    run alone"""
+    from ymc3d_b200.workloads import uneven
+    w = uneven(ngeoms=64, photons=10_000, max_dim=72)
+    assert sum(3 * 16 * p.num_tissue_types for p in w.props) + 64 * 72 + 28672 > 48 * 1024
+    together = m.run(w.geoms, w.props, w.jobs, table=table)
+    for k in (0, 17, 63):
+        job = w.jobs[k]
+        alone = m.run([w.geoms[job.geom]], [w.props[job.props]],
+                      [m.Job(0, 0, job.photons, job.seed, job.beam)], table=table)[0]
+        assert together[k].totals == alone.totals
+        assert np.array_equal(together[k].drs, alone.drs)
+
+
 def test_plan_reexecute_identical(table):
     g, p = layered_small()
     plan = m.Plan([g], [p], [m.Job(0, 0, 200_000, 9, "uniform")], table=table)

@@ -17,8 +17,10 @@ from pathlib import Path
 
 from . import HERE, Job, Plan, default_table
 
-# (threads per block, blocks per SM; 0 = as many as fit)
-CANDIDATES = ((256, 0), (128, 0), (64, 0))
+# (threads per block, blocks per SM; 0 = as many as fit).  Each block holds 28 KB of
+# per-thread tally columns sized for 256 threads, so blocks below 128 threads run
+# out of shared memory before they fill an SM's 768 threads.
+CANDIDATES = ((256, 0), (128, 0))
 _CACHE_FILE = HERE / "_data" / "tuning.json"
 _cache: dict | None = None
 
@@ -67,7 +69,7 @@ def _sample_jobs(jobs, streams_per_job: int):
 
 
 def tune(geoms, props, jobs, table=None, math: str = "fast", device: int = 0,
-         candidates=CANDIDATES, sample_streams: int = 0, reps: int = 1,
+         candidates=CANDIDATES, sample_streams: int = 0, reps: int = 2,
          use_cache: bool = True, steps: str = "merged") -> dict:
     """Return {"block", "blocks_per_sm", "ms", "table"} for the fastest candidate."""
     import torch

@@ -47,7 +47,9 @@ int fail(int code, const char *fmt, ...)
             return fail(MC3D_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));             \
     } while (0)
 
-const int kMaxSharedTable = 200 * 1024; /* bytes of optical tables per launch */
+/* bytes of optical tables and geometry descriptors per launch (shared memory:
+ * 227 KB per block, less 28 KB of tally columns) */
+const int kMaxSharedTable = 192 * 1024;
 const int64_t kMaxAttempts = 4096;       /* seeding attempts per stream before giving up */
 
 /* seeding-generator constants for multiplier `begin` (see mc3d_rng.h) */
@@ -143,7 +145,7 @@ struct mc3d_plan {
     int64_t total_bins = 0;
     int64_t total_photons = 0;
     std::vector<uint8_t *> d_grids;
-    std::vector<uint8_t *> d_radius; /* safe-distance maps (merged steps) */
+    std::vector<uint16_t *> d_cells; /* packed tissue | safe distance (merged steps) */
     bool jump = false;
     JobDev *d_jobs = nullptr;
     GeomDev *d_geoms = nullptr;
@@ -173,7 +175,7 @@ static void plan_free(mc3d_plan *p)
     cudaSetDevice(p->device);
     if (p->stream) cudaStreamSynchronize(p->stream);
     for (uint8_t *g : p->d_grids) cudaFree(g);
-    for (uint8_t *r : p->d_radius) cudaFree(r);
+    for (uint16_t *r : p->d_cells) cudaFree(r);
     cudaFree(p->d_jobs);
     cudaFree(p->d_geoms);
     cudaFree(p->d_props);
@@ -252,9 +254,11 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         props_offset[i] = entries;
         entries += 3 * p.num_tissue_types;
     }
-    if ((int64_t)entries * 16 > kMaxSharedTable)
-        return fail(MC3D_ERR_CAPACITY, "optical tables need %d bytes of shared memory (max %d)",
-                    entries * 16, kMaxSharedTable);
+    if ((int64_t)entries * 16 + (int64_t)ngeoms * (int64_t)sizeof(GeomDev) > kMaxSharedTable)
+        return fail(MC3D_ERR_CAPACITY,
+                    "optical tables and geometry descriptors need %lld bytes of shared memory "
+                    "(max %d)", (long long)entries * 16 + (long long)ngeoms * sizeof(GeomDev),
+                    kMaxSharedTable);
 
     mc3d_seed_consts sc;
     make_seed_consts(table[0], &sc);
@@ -377,17 +381,22 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         d.tissue = p->d_grids[i];
     }
     if (p->jump) {
-        p->d_radius.assign(ngeoms, nullptr);
+        /* per geometry: the safe-distance map into scratch, then packed with the
+         * tissue into 16-bit cells (scratch: two pass buffers and the map) */
+        p->d_cells.assign(ngeoms, nullptr);
         uint8_t *tmp = nullptr;
-        PLAN_TRY(cudaMalloc(&tmp, 2 * max_map));
+        PLAN_TRY(cudaMalloc(&tmp, 3 * max_map));
         cudaError_t e = cudaSuccess;
         for (int i = 0; i < ngeoms && e == cudaSuccess; i++) {
             size_t nmap = (size_t)geoms[i].nx * geoms[i].ny * (geoms[i].nz + MC3D_SAFE_CAP);
-            e = cudaMalloc(&p->d_radius[i], nmap);
+            e = cudaMalloc(&p->d_cells[i], 2 * nmap);
             if (e == cudaSuccess)
                 e = launch_safe_distance(p->d_grids[i], geoms[i].nx, geoms[i].ny, geoms[i].nz,
-                                         p->d_radius[i], tmp, tmp + max_map, p->stream);
-            gh[i].radius = p->d_radius[i];
+                                         tmp + 2 * max_map, tmp, tmp + max_map, p->stream);
+            if (e == cudaSuccess)
+                e = launch_pack_cells(p->d_grids[i], tmp + 2 * max_map, geoms[i].nx, geoms[i].ny,
+                                      geoms[i].nz, p->d_cells[i], p->stream);
+            gh[i].cells = p->d_cells[i];
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
         cudaFree(tmp);
@@ -472,12 +481,25 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     cudaDeviceProp prop;
     PLAN_TRY(cudaGetDeviceProperties(&prop, p->device));
     p->block = opt.block ? opt.block : 256;
-    p->smem = sizeof(float4) * entries;
-    if (p->smem > 48 * 1024) {
-        PLAN_TRY(p->math == MC3D_MATH_FAST ? smem_limit_photon_fast(p->smem)
-                                          : smem_limit_photon_exact(p->smem));
+    p->smem = sizeof(float4) * entries + sizeof(GeomDev) * ngeoms;
+    /* The kernels' static shared memory (28 KB of per-thread tallies) counts
+     * against the 48 KB a block gets without opting in, so the kernels always opt
+     * in, to the device's whole per-block limit: the attribute is per function,
+     * and a lower value would break a live plan that needs more. */
+    {
+        cudaFuncAttributes fa;
+        PLAN_TRY(p->math == MC3D_MATH_FAST ? attributes_photon_fast(&fa)
+                                          : attributes_photon_exact(&fa));
+        const size_t max_dyn = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
+        if (p->smem > max_dyn) {
+            plan_free(p);
+            return fail(MC3D_ERR_CAPACITY, "optical tables and geometry descriptors need %zu B "
+                        "of shared memory, the device allows %zu", p->smem, max_dyn);
+        }
+        PLAN_TRY(p->math == MC3D_MATH_FAST ? smem_limit_photon_fast(max_dyn)
+                                          : smem_limit_photon_exact(max_dyn));
     }
-    p->variant = p->jump ? 0 : MC3D_VARIANT_VOXEL_STEPS;
+    p->variant = (p->jump ? 0 : MC3D_VARIANT_VOXEL_STEPS) | (ngeoms == 1 ? MC3D_VARIANT_ONE_GEOM : 0);
     int bps = 0;
     PLAN_TRY(p->math == MC3D_MATH_FAST ? occupancy_photon_fast(p->block, p->smem, &bps, p->variant)
                                       : occupancy_photon_exact(p->block, p->smem, &bps));
@@ -492,6 +514,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     memset(&P, 0, sizeof P);
     P.jobs = p->d_jobs;
     P.geoms = p->d_geoms;
+    P.geom0 = gh[0];
     P.props_table = p->d_props;
     P.multipliers = p->d_mult;
     P.rejections = p->d_rej;
@@ -507,6 +530,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     P.total_streams = stream_base;
     P.max_steps = opt.max_steps > 0 ? std::min<int64_t>(opt.max_steps, INT32_MAX) : (1 << 24);
     P.njobs = njobs;
+    P.ngeoms = ngeoms;
     P.props_entries = entries;
     P.seed = sc;
     PLAN_TRY(cudaStreamSynchronize(p->stream));

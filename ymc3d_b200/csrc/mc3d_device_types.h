@@ -27,7 +27,7 @@ struct GeomDev {
     float rdx, rdy, rdz;   /* 1 / voxel size (fast math only) */
     float pad2;
     const uint8_t *tissue; /* nz*ny*nx, x fastest; 0 = air */
-    const uint8_t *radius; /* safe-distance map, nz + MC3D_SAFE_CAP slices (merged steps) */
+    const uint16_t *cells; /* tissue | safe distance << 8, nz + MC3D_SAFE_CAP slices (merged) */
 };
 
 struct JobDev {
@@ -85,7 +85,11 @@ struct KernelParams {
     int64_t max_steps;
     int32_t njobs;
     int32_t props_entries;
+    int32_t ngeoms;
+    int32_t pad_geoms;
     mc3d_seed_consts seed;
+    GeomDev geom0; /* the only geometry of a one-geometry launch, read from the
+                      parameter space instead of being copied per thread */
 };
 
 } /* namespace mc3d */

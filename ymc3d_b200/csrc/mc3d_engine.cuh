@@ -111,7 +111,8 @@ static __device__ __forceinline__ int grid_coord(float x, float ux, float d, flo
 }
 
 /* src/mc3d_gpu.cu:24-27 with the clamp addressing of the texture (:416-418).
- * With JUMP the voxel's safe distance rides in bits 8-15 of the result (0 above
+ * With JUMP the lookup reads the packed map (tissue | safe distance << 8, one
+ * 16-bit load), so the safe distance rides in bits 8-15 of the result (0 above
  * the surface, where the tissue is air). */
 template <bool JUMP = false>
 static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, int k, float z,
@@ -120,11 +121,12 @@ static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, 
     int ci = min(max(i, 0), g.nx - 1);
     int cj = min(max(j, 0), g.ny - 1);
     int ck = min(max(k, 0), g.nz - 1);
-    const int64_t col = (int64_t)cj * g.nx + ci;
-    int t = __ldg(g.tissue + (int64_t)ck * g.ny * g.nx + col);
+    int t;
     if (JUMP) {
         const int rk = min(max(k, 0), g.nz - 1 + MC3D_SAFE_CAP);
-        t |= (int)__ldg(g.radius + (int64_t)rk * g.ny * g.nx + col) << 8;
+        t = __ldg(g.cells + ((int64_t)rk * g.ny + cj) * g.nx + ci);
+    } else {
+        t = __ldg(g.tissue + ((int64_t)ck * g.ny + cj) * g.nx + ci);
     }
     return ((z <= 0) && (uz < 0)) ? MC3D_TISSUE_AIR : t;
 }
@@ -206,14 +208,11 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     /* per tissue: (mua, mus, g, n), (mu_t, mua/mu_t, 1/mu_t, 1/(2g)),
      * (1-g^2, 1-g, 2g, 1+g^2) -- each the float the reference computes per step */
     const int tis = JUMP ? (p.tissue & 0xff) : p.tissue;
-    const float4 t0 = tab[MC3D_TAB_STRIDE * tis];
-    const float4 t1 = tab[MC3D_TAB_STRIDE * tis + 1];
-    const float4 t2 = tab[MC3D_TAB_STRIDE * tis + 2];
-    float ni = t0.w;
+    const float4 *tt = tab + MC3D_TAB_STRIDE * tis;
+    float ni = tt[0].w;
     float nt = ni;
-    float mu_a = t0.x;
-    float mu_t = t1.x;
-    (void)mu_a;
+    const float mu_t = tt[1].x;
+    const float rmu_t = tt[1].z;
 
     float newx = p.x, newy = p.y, newz = p.z;
     int axes = 0;
@@ -222,9 +221,9 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
 
     bool hit = db * mu_t <= p.s;
     float ds = hit ? db * mu_t : p.s;
-    newx = hit ? newx : p.x + M::div_r(p.ux * ds, mu_t, t1.z);
-    newy = hit ? newy : p.y + M::div_r(p.uy * ds, mu_t, t1.z);
-    newz = hit ? newz : p.z + M::div_r(p.uz * ds, mu_t, t1.z);
+    newx = hit ? newx : p.x + M::div_r(p.ux * ds, mu_t, rmu_t);
+    newy = hit ? newy : p.y + M::div_r(p.uy * ds, mu_t, rmu_t);
+    newz = hit ? newz : p.z + M::div_r(p.uz * ds, mu_t, rmu_t);
     float s = p.s - ds;
 
     int nexti = grid_coord<M>(newx, p.ux, g.dx, g.rdx);
@@ -300,7 +299,7 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
 
     /* absorption, src/mc3d_gpu.cu:262-263 */
     float W = p.W;
-    float dW = (mu_t > 0) ? t1.y * W : 0;
+    float dW = (mu_t > 0) ? tt[1].y * W : 0;
     float W_before = W;
     W = W - dW * (float)(!hit);
     if (AMAP && !hit && mu_t > 0) {
@@ -335,8 +334,9 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     }
 
     /* Henyey-Greenstein, src/mc3d_gpu.cu:282-294 */
+    const float4 t2 = tt[2];
     float costheta = M::div(t2.x, t2.y + t2.z * mc3d_rand_oc(&rx, ra));
-    costheta = t1.w * (t2.w - costheta * costheta);
+    costheta = tt[1].w * (t2.w - costheta * costheta);
     float sintheta = M::sqrt(1 - costheta * costheta);
     float phi_divpi = 2 * mc3d_rand_co(&rx, ra);
     float cosphi, sinphi;
@@ -516,18 +516,23 @@ static __device__ __forceinline__ uint64_t stream_seed(const KernelParams &P, co
 
 /* The persistent photon loop.  JUMP selects merged steps (photon_step) and needs
  * every geometry's safe-distance map. */
-template <class M, bool AMAP, bool JUMP = false>
+template <class M, bool AMAP, bool JUMP = false, bool ONE_GEOM = false>
 __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
 {
+    /* dynamic shared memory: the optical tables, then (several geometries) the
+     * geometry descriptors, read from there instead of being held per thread */
     extern __shared__ float4 sh_tab[];
     __shared__ unsigned long long sh_acc[MC3D_NUM_TOTALS * MC3D_MAX_BLOCK];
     for (int t = threadIdx.x; t < P.props_entries; t += blockDim.x) sh_tab[t] = P.props_table[t];
+    GeomDev *sh_geom = reinterpret_cast<GeomDev *>(sh_tab + P.props_entries);
+    if (!ONE_GEOM)
+        for (int t = threadIdx.x; t < P.ngeoms; t += blockDim.x) sh_geom[t] = P.geoms[t];
     const Acc acc{sh_acc + threadIdx.x};
     acc_clear(acc);
     __syncthreads();
 
     int job = -1;
-    GeomDev g;
+    const GeomDev *gp = sh_geom;
     const float4 *tab = sh_tab;
     int64_t left = 0, local = 0;
     uint64_t rx = 0;
@@ -550,7 +555,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
                 if (gs >= P.total_streams) break;
                 job = find_job(P.jobs, P.njobs, gs);
                 const JobDev &jb = P.jobs[job];
-                g = P.geoms[jb.geom];
+                gp = sh_geom + jb.geom;
                 tab = sh_tab + jb.props_offset;
                 if (AMAP) amap = P.amap + jb.amap_offset;
                 local = gs - jb.stream_base + jb.stream_first;
@@ -559,6 +564,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
                 rx = stream_seed(P, jb, local, ra);
                 if (left == 0) continue;
             }
+            const GeomDev &g = ONE_GEOM ? P.geom0 : *gp;
             /* photontrack_reinitialize, src/mc3d_gpu.cu:74-111 */
             if (P.jobs[job].beam == 0) {
                 p.x = g.Lx * mc3d_rand_co(&rx, ra);
@@ -584,6 +590,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
             left--;
         }
 
+        const GeomDev &g = ONE_GEOM ? P.geom0 : *gp;
         float db;
         bool lat_mirror;
         bool froze;

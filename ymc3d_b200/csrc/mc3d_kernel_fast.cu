@@ -8,7 +8,12 @@
 
 namespace mc3d {
 
-/* merged steps (safe-distance jumps through uniform tissue) */
+/* Eight instantiations: merged steps (box DDA over uniform cubes) or one step
+ * per voxel face; with or without the absorption map; several geometries (their
+ * descriptors in shared memory) or one (its descriptor read from the kernel
+ * parameters, which keeps it out of the registers). */
+
+/* merged steps */
 __global__ void __launch_bounds__(256, 3) photon_kernel_fast(const __grid_constant__ KernelParams P)
 {
     photon_kernel_body<MathFast, false, true>(P);
@@ -34,11 +39,39 @@ __global__ void __launch_bounds__(256, 3)
     photon_kernel_body<MathFast, true, false>(P);
 }
 
+/* one geometry */
+__global__ void __launch_bounds__(256, 3) photon_kernel_fast_g1(const __grid_constant__ KernelParams P)
+{
+    photon_kernel_body<MathFast, false, true, true>(P);
+}
+
+__global__ void __launch_bounds__(256, 3)
+    photon_kernel_fast_amap_g1(const __grid_constant__ KernelParams P)
+{
+    photon_kernel_body<MathFast, true, true, true>(P);
+}
+
+__global__ void __launch_bounds__(256, 3)
+    photon_kernel_fast_voxel_g1(const __grid_constant__ KernelParams P)
+{
+    photon_kernel_body<MathFast, false, false, true>(P);
+}
+
+__global__ void __launch_bounds__(256, 3)
+    photon_kernel_fast_voxel_amap_g1(const __grid_constant__ KernelParams P)
+{
+    photon_kernel_body<MathFast, true, false, true>(P);
+}
+
 typedef void (*photon_kernel_t)(KernelParams);
 
 static photon_kernel_t pick(bool amap, int variant)
 {
     const bool voxel = (variant & MC3D_VARIANT_VOXEL_STEPS) != 0;
+    if (variant & MC3D_VARIANT_ONE_GEOM) {
+        if (amap) return voxel ? photon_kernel_fast_voxel_amap_g1 : photon_kernel_fast_amap_g1;
+        return voxel ? photon_kernel_fast_voxel_g1 : photon_kernel_fast_g1;
+    }
     if (amap) return voxel ? photon_kernel_fast_voxel_amap : photon_kernel_fast_amap;
     return voxel ? photon_kernel_fast_voxel : photon_kernel_fast;
 }
@@ -58,8 +91,10 @@ cudaError_t occupancy_photon_fast(int block, size_t smem, int *blocks_per_sm, in
 
 cudaError_t smem_limit_photon_fast(size_t smem)
 {
-    const photon_kernel_t all[] = {photon_kernel_fast, photon_kernel_fast_amap,
-                                   photon_kernel_fast_voxel, photon_kernel_fast_voxel_amap};
+    const photon_kernel_t all[] = {photon_kernel_fast,          photon_kernel_fast_amap,
+                                   photon_kernel_fast_voxel,    photon_kernel_fast_voxel_amap,
+                                   photon_kernel_fast_g1,       photon_kernel_fast_amap_g1,
+                                   photon_kernel_fast_voxel_g1, photon_kernel_fast_voxel_amap_g1};
     for (photon_kernel_t k : all) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);

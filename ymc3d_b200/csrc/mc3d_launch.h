@@ -16,6 +16,8 @@ namespace mc3d {
  * 80-register one and is not built: one kernel serves every launch shape, so the
  * tallies cannot depend on the shape.) */
 #define MC3D_VARIANT_VOXEL_STEPS 2
+/* one geometry in the launch: its descriptor is read from the kernel parameters */
+#define MC3D_VARIANT_ONE_GEOM 4
 cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_t smem,
                                cudaStream_t stream, int variant);
 cudaError_t launch_photon_exact(const KernelParams &P, int grid, int block, size_t smem,
@@ -38,6 +40,8 @@ cudaError_t launch_seed_dump(const KernelParams &P, int64_t first, int64_t count
  * nx * ny * (nz + MC3D_SAFE_CAP) bytes each */
 cudaError_t launch_safe_distance(const uint8_t *tissue, int nx, int ny, int nz, uint8_t *out,
                                  uint8_t *tmp_a, uint8_t *tmp_b, cudaStream_t stream);
+cudaError_t launch_pack_cells(const uint8_t *tissue, const uint8_t *radius, int nx, int ny, int nz,
+                              uint16_t *cells, cudaStream_t stream);
 cudaError_t launch_mwc_draws(const uint64_t *x, const uint32_t *a, int64_t ngen, int64_t n,
                              float *out, cudaStream_t stream);
 

@@ -64,10 +64,11 @@ static_assert(sizeof(JobDev) <= 256 && sizeof(GeomDev) <= 256, "descriptor slots
 /* the scratch: one per GPU that loads the library, alive until exit */
 static __device__ __align__(256) unsigned char g_noalloc_scratch[MC3D_NOALLOC_SCRATCH_BYTES];
 
+/* one geometry, per-face steps; the descriptor is read from P.geom0 */
 __global__ void __launch_bounds__(256, 3)
     photon_kernel_noalloc(const __grid_constant__ KernelParams P)
 {
-    photon_kernel_body<MathFast, false>(P);
+    photon_kernel_body<MathFast, false, false, true>(P);
 }
 
 /* largest tissue index of the device-resident grid, into a scratch word */
@@ -237,6 +238,7 @@ extern "C" int mc3d_run_noalloc(const mc3d_geom *geom, const mc3d_props *props,
     memset(&P, 0, sizeof P);
     P.jobs = (const JobDev *)(base + kOffJob);
     P.geoms = (const GeomDev *)(base + kOffGeom);
+    P.geom0 = gd;
     P.props_table = (const float4 *)(base + kOffProps);
     P.multipliers = (const uint32_t *)(base + kOffMult);
     P.rejections = (const RejectionDev *)(base + kOffRej);

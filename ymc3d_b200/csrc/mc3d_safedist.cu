@@ -97,6 +97,18 @@ __global__ void pass_minmax_kernel(const uint8_t *__restrict__ in, int nx, int n
     }
 }
 
+__global__ void pack_kernel(const uint8_t *__restrict__ t, const uint8_t *__restrict__ r, int nx,
+                            int ny, int nz, int nz_map, uint16_t *__restrict__ out)
+{
+    const int64_t plane = (int64_t)nx * ny;
+    const int64_t nv = plane * nz_map;
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(v / plane);
+        out[v] = (uint16_t)(t[(int64_t)min(k, nz - 1) * plane + v % plane] | ((int)r[v] << 8));
+    }
+}
+
 int grid_for(int64_t nv)
 {
     int64_t want = (nv + 255) / 256;
@@ -116,6 +128,16 @@ cudaError_t launch_safe_distance(const uint8_t *tissue, int nx, int ny, int nz, 
     pass_x_kernel<<<grid, 256, 0, stream>>>(tmp_a, nx, ny, nz_map, tmp_b);
     pass_minmax_kernel<<<grid, 256, 0, stream>>>(tmp_b, nx, ny, nz_map, 1, tmp_a);
     pass_minmax_kernel<<<grid, 256, 0, stream>>>(tmp_a, nx, ny, nz_map, 2, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_cells(const uint8_t *tissue, const uint8_t *radius, int nx, int ny, int nz,
+                              uint16_t *cells, cudaStream_t stream)
+{
+    const int nz_map = nz + MC3D_SAFE_CAP;
+    const int64_t nv = (int64_t)nx * ny * nz_map;
+    if (nx <= 0 || ny <= 0 || nz <= 0) return cudaSuccess;
+    pack_kernel<<<grid_for(nv), 256, 0, stream>>>(tissue, radius, nx, ny, nz, nz_map, cells);
     return cudaGetLastError();
 }
 
