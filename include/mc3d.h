@@ -46,7 +46,12 @@ enum mc3d_status {
 };
 
 enum mc3d_beam { MC3D_BEAM_UNIFORM = 0, MC3D_BEAM_PENCIL = 1 };
-enum mc3d_math { MC3D_MATH_FAST = 0, MC3D_MATH_EXACT = 1 };
+/* FAST: FP32 with the GPU's approximate division, sqrt, log and sin, as the
+ * reference's -use_fast_math build.  EXACT: FP32 with IEEE operations and
+ * reproducible series functions, bit-identical to the CPU transcription.  F64:
+ * the same loop stepping in FP64, the precision reference (no counterpart in the
+ * reference). */
+enum mc3d_math { MC3D_MATH_FAST = 0, MC3D_MATH_EXACT = 1, MC3D_MATH_F64 = 2 };
 
 /* Step decomposition of the fast-math kernel.  MERGED (the default) replaces the
  * voxel-face crossings of a flight through uniform tissue by one step to the

@@ -2,7 +2,6 @@
 from __future__ import annotations
 
 import numpy as np
-from scipy import stats
 
 import oracle
 import ymc3d_b200 as m
@@ -23,35 +22,8 @@ def residual(t: dict) -> int:
                                    int(t["rr_created"]) + int(t["lost"]))
 
 
-def superbin(a: np.ndarray, f: int) -> np.ndarray:
-    ny, nx = a.shape
-    return a[: ny - ny % f, : nx - nx % f].reshape(ny // f, f, nx // f, f).sum(axis=(1, 3))
-
-
-def drs_chi2(sum_a, sq_a, n_a, sum_b, sq_b, n_b, f=8, min_mean=1e-5):
-    """Chi-square of per-(super)bin reflectance R = sum W / N between two runs,
-    each bin's variance from its own sum W^2: returns (chi2, dof, p)."""
-    sa = superbin(sum_a.astype(np.float64), f) / m.WEIGHT_SCALE
-    qa = superbin(sq_a.astype(np.float64), f) / m.WEIGHT_SCALE
-    sb = superbin(sum_b.astype(np.float64), f) / m.WEIGHT_SCALE
-    qb = superbin(sq_b.astype(np.float64), f) / m.WEIGHT_SCALE
-    ra, rb = sa / n_a, sb / n_b
-    va = np.maximum(qa / n_a - ra ** 2, 0) / n_a
-    vb = np.maximum(qb / n_b - rb ** 2, 0) / n_b
-    ok = ((ra + rb) / 2 > min_mean) & (va + vb > 0)
-    chi2 = float(np.sum((ra[ok] - rb[ok]) ** 2 / (va[ok] + vb[ok])))
-    dof = int(ok.sum())
-    return chi2, dof, float(stats.chi2.sf(chi2, dof)) if dof else 1.0
-
-
-def total_z(ta: dict, tb: dict, key="r_in"):
-    """z-score of a total weight fraction between two runs (binomial-like variance
-    bounded by the per-photon weight <= 1)."""
-    fa = ta[key] / m.WEIGHT_SCALE / ta["photons"]
-    fb = tb[key] / m.WEIGHT_SCALE / tb["photons"]
-    va = fa * (1 - min(fa, 1)) / ta["photons"] + 1e-30
-    vb = fb * (1 - min(fb, 1)) / tb["photons"] + 1e-30
-    return (fa - fb) / np.sqrt(va + vb)
+# the comparison statistics live in the package (bench.py uses them too)
+from ymc3d_b200.stats import drs_chi2, superbin, total_z  # noqa: E402,F401
 
 
 def safe_distance_bruteforce(t: np.ndarray, cap: int = 63) -> np.ndarray:

@@ -31,7 +31,7 @@ STATUS_NAMES = {
     -11: "MC3D_ERR_CAPACITY", -12: "MC3D_ERR_CANCELLED",
 }
 BEAMS = {"uniform": 0, "pencil": 1}
-MATH = {"fast": 0, "exact": 1}
+MATH = {"fast": 0, "exact": 1, "f64": 2}
 STEPS = {"merged": 0, "voxel": 1}
 TOTAL_FIELDS = ("photons", "steps", "w_launched", "r_in", "r_out", "t_in", "t_out", "absorbed",
                 "rr_killed", "rr_created", "lost", "capped", "quickfix", "fresnel")

@@ -30,6 +30,8 @@ UNITS = {
     "mc3d_kernel_fast.cu": ["-use_fast_math", "-Xptxas", "-v"],
     "mc3d_kernel_exact.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
                              "-Xptxas", "-v"],
+    "mc3d_kernel_f64.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
+                           "-Xptxas", "-v"],
     "mc3d_seed.cu": ["-fmad=false"],
     "mc3d_safedist.cu": [],
     "mc3d_api.cu": ["-fmad=false", "-Xcompiler", "-ffp-contract=off"],

@@ -5,7 +5,7 @@
  * Same inputs, same stdout/stderr lines and the same outname_drs.bin and
  * outname_simparam.dat.  The third argument, ignored by the reference
  * (README.md:38), is read as an optional key=value file:
- *   photons=30000000  seed=<time>  beam=uniform|pencil  streams=0  math=fast|exact
+ *   photons=30000000  seed=<time>  beam=uniform|pencil  streams=0  math=fast|exact|f64
  *   safeprimes=safeprimes_base32.txt  max_steps=0  device=0  abs_map=0  save_trans=0
  *   steps=merged|voxel (fast math: merged crossings in uniform tissue, or one step
  *   per voxel face like the reference)
@@ -64,7 +64,8 @@ bool read_params(const char *path, Params &p)
         else if (k == "seed") { p.seed = std::stoull(v); p.seed_set = true; }
         else if (k == "beam") p.beam = (v == "pencil") ? MC3D_BEAM_PENCIL : MC3D_BEAM_UNIFORM;
         else if (k == "streams") p.streams = std::stoll(v);
-        else if (k == "math") p.math = (v == "exact") ? MC3D_MATH_EXACT : MC3D_MATH_FAST;
+        else if (k == "math")
+            p.math = (v == "exact") ? MC3D_MATH_EXACT : (v == "f64") ? MC3D_MATH_F64 : MC3D_MATH_FAST;
         else if (k == "steps") p.steps = (v == "voxel") ? MC3D_STEPS_VOXEL : MC3D_STEPS_MERGED;
         else if (k == "safeprimes") p.safeprimes = v;
         else if (k == "max_steps") p.max_steps = std::stoll(v);

@@ -219,7 +219,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     mc3d_options opt;
     if (opt_in) opt = *opt_in;
     else mc3d_default_options(&opt);
-    if (opt.math != MC3D_MATH_FAST && opt.math != MC3D_MATH_EXACT)
+    if (opt.math != MC3D_MATH_FAST && opt.math != MC3D_MATH_EXACT && opt.math != MC3D_MATH_F64)
         return fail(MC3D_ERR_ARG, "unknown math mode %d", opt.math);
     if (opt.steps != MC3D_STEPS_MERGED && opt.steps != MC3D_STEPS_VOXEL)
         return fail(MC3D_ERR_ARG, "unknown step mode %d", opt.steps);
@@ -488,21 +488,24 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
      * and a lower value would break a live plan that needs more. */
     {
         cudaFuncAttributes fa;
-        PLAN_TRY(p->math == MC3D_MATH_FAST ? attributes_photon_fast(&fa)
-                                          : attributes_photon_exact(&fa));
+        PLAN_TRY(p->math == MC3D_MATH_FAST    ? attributes_photon_fast(&fa)
+                 : p->math == MC3D_MATH_EXACT ? attributes_photon_exact(&fa)
+                                              : attributes_photon_f64(&fa));
         const size_t max_dyn = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
         if (p->smem > max_dyn) {
             plan_free(p);
             return fail(MC3D_ERR_CAPACITY, "optical tables and geometry descriptors need %zu B "
                         "of shared memory, the device allows %zu", p->smem, max_dyn);
         }
-        PLAN_TRY(p->math == MC3D_MATH_FAST ? smem_limit_photon_fast(max_dyn)
-                                          : smem_limit_photon_exact(max_dyn));
+        PLAN_TRY(p->math == MC3D_MATH_FAST    ? smem_limit_photon_fast(max_dyn)
+                 : p->math == MC3D_MATH_EXACT ? smem_limit_photon_exact(max_dyn)
+                                              : smem_limit_photon_f64(max_dyn));
     }
     p->variant = (p->jump ? 0 : MC3D_VARIANT_VOXEL_STEPS) | (ngeoms == 1 ? MC3D_VARIANT_ONE_GEOM : 0);
     int bps = 0;
     PLAN_TRY(p->math == MC3D_MATH_FAST ? occupancy_photon_fast(p->block, p->smem, &bps, p->variant)
-                                      : occupancy_photon_exact(p->block, p->smem, &bps));
+             : p->math == MC3D_MATH_EXACT ? occupancy_photon_exact(p->block, p->smem, &bps)
+                                          : occupancy_photon_f64(p->block, p->smem, &bps));
     if (bps <= 0) {
         plan_free(p);
         return fail(MC3D_ERR_CAPACITY, "kernel does not fit an SM with block %d", opt.block);
@@ -548,7 +551,9 @@ static int plan_enqueue(mc3d_plan *p, cudaStream_t s)
         CUDA_TRY(cudaMemsetAsync(p->d_amap, 0, sizeof(unsigned long long) * p->total_voxels, s));
     if (p->math == MC3D_MATH_FAST)
         CUDA_TRY(launch_photon_fast(p->P, p->grid, p->block, p->smem, s, p->variant));
-    else CUDA_TRY(launch_photon_exact(p->P, p->grid, p->block, p->smem, s));
+    else if (p->math == MC3D_MATH_EXACT)
+        CUDA_TRY(launch_photon_exact(p->P, p->grid, p->block, p->smem, s));
+    else CUDA_TRY(launch_photon_f64(p->P, p->grid, p->block, p->smem, s));
     return MC3D_OK;
 }
 

@@ -32,8 +32,40 @@
 
 namespace mc3d {
 
-/* ---------------------------------------------------------------- math policies */
-struct MathExact {
+/* ---------------------------------------------------------------- math policies
+ * A policy fixes the transport arithmetic type (real) and how the elementary
+ * operations are evaluated, and reads the per-tissue coefficients of the optical
+ * table (three float4 per tissue, see photon_step). */
+
+/* The FP32 policies read every coefficient as the float the reference computes
+ * per step, precomputed on the host. */
+struct FloatTable {
+    using real = float;
+    static __device__ __forceinline__ float n(const float4 *tt) { return tt[0].w; }
+    static __device__ __forceinline__ float mu_t(const float4 *tt) { return tt[1].x; }
+    static __device__ __forceinline__ float albedo_c(const float4 *tt) { return tt[1].y; }
+    static __device__ __forceinline__ float rmu_t(const float4 *tt) { return tt[1].z; }
+    /* Henyey-Greenstein cos(theta) for the draw xi in (0, 1] (src/mc3d_gpu.cu:282-286) */
+    template <class M>
+    static __device__ __forceinline__ float hg_cos(const float4 *tt, float xi)
+    {
+        const float4 t2 = tt[2];
+        float c = M::div(t2.x, t2.y + t2.z * xi);
+        return tt[1].w * (t2.w - c * c);
+    }
+    /* thresholds of src/mc3d_types.h:11-18, see the constants below */
+    static __device__ __forceinline__ bool w_below_threshold(float w) { return w <= 0x1.a36e2ep-14f; }
+    static __device__ __forceinline__ bool uz_within(float u) { return u <= 0x1.fffeb0p-1f; }
+    static __device__ __forceinline__ float roulette_survivor(float w)
+    {
+        return (float)((double)w / 0.1);
+    }
+    static __device__ __forceinline__ float zero_threshold() { return (float)(1 - 0.99999); }
+    /* fixed-point weight, 2^-32 resolution */
+    static __device__ __forceinline__ uint64_t qw(float w) { return __float2ull_rn(w * 4294967296.0f); }
+};
+
+struct MathExact : FloatTable {
     static constexpr bool kFast = false;
     static __device__ __forceinline__ float div(float a, float b) { return a / b; }
     /* a / b where the caller also holds r = 1/b: the exact policy divides */
@@ -47,11 +79,15 @@ struct MathExact {
     {
         mc3d_xm_sincospif(x, s, c);
     }
+    static __device__ __forceinline__ float floor(float x) { return floorf(x); }
+    static __device__ __forceinline__ float fmin(float a, float b) { return fminf(a, b); }
+    static __device__ __forceinline__ float fabs(float x) { return fabsf(x); }
+    static __device__ __forceinline__ float copysign(float a, float b) { return copysignf(a, b); }
 };
 
 /* Compiled only in a translation unit built with -use_fast_math, where the
  * operators and functions below map to the approximate hardware paths. */
-struct MathFast {
+struct MathFast : FloatTable {
     static constexpr bool kFast = true;
     /* every denominator divided here is a direction cosine, a sum of products of
      * cosines and sines, a refractive-index sum or 1 - g + 2 g xi, all far below the
@@ -70,6 +106,60 @@ struct MathFast {
         __sincosf(3.14159265358979f * (x - 1.0f), &sn, &cs);
         *s = -sn;
         *c = -cs;
+    }
+    static __device__ __forceinline__ float floor(float x) { return floorf(x); }
+    static __device__ __forceinline__ float fmin(float a, float b) { return fminf(a, b); }
+    static __device__ __forceinline__ float fabs(float x) { return fabsf(x); }
+    static __device__ __forceinline__ float copysign(float a, float b) { return copysignf(a, b); }
+};
+
+/* FP64 stepping: the same loop with every transport quantity in double, the
+ * coefficients derived in double from the table's float (mua, mus, g, n), and
+ * the reference's double literals compared in double.  Random numbers stay the
+ * reference's 32-bit draws.  Built with IEEE division and square root; the
+ * precision reference for the FP32 policies. */
+struct MathF64 {
+    using real = double;
+    static constexpr bool kFast = false;
+    static __device__ __forceinline__ double div(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double div_r(double a, double b, double) { return a / b; }
+    static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+    static __device__ __forceinline__ double rsqrt(double x) { return 1.0 / ::sqrt(x); }
+    static __device__ __forceinline__ double log(double x) { return ::log(x); }
+    static __device__ __forceinline__ double acos(double x) { return ::acos(x); }
+    static __device__ __forceinline__ double sin(double x) { return ::sin(x); }
+    static __device__ __forceinline__ void sincospi(double x, double *s, double *c)
+    {
+        ::sincospi(x, s, c);
+    }
+    static __device__ __forceinline__ double floor(double x) { return ::floor(x); }
+    static __device__ __forceinline__ double fmin(double a, double b) { return ::fmin(a, b); }
+    static __device__ __forceinline__ double fabs(double x) { return ::fabs(x); }
+    static __device__ __forceinline__ double copysign(double a, double b) { return ::copysign(a, b); }
+    static __device__ __forceinline__ double n(const float4 *tt) { return tt[0].w; }
+    static __device__ __forceinline__ double mu_t(const float4 *tt)
+    {
+        return (double)tt[0].x + (double)tt[0].y;
+    }
+    static __device__ __forceinline__ double albedo_c(const float4 *tt)
+    {
+        return (double)tt[0].x / mu_t(tt);
+    }
+    static __device__ __forceinline__ double rmu_t(const float4 *tt) { return 1.0 / mu_t(tt); }
+    template <class M>
+    static __device__ __forceinline__ double hg_cos(const float4 *tt, double xi)
+    {
+        const double g = tt[0].z;
+        const double c = (1 - g * g) / (1 - g + 2 * g * xi);
+        return (1 + g * g - c * c) / (2 * g);
+    }
+    static __device__ __forceinline__ bool w_below_threshold(double w) { return w < 0.0001; }
+    static __device__ __forceinline__ bool uz_within(double u) { return u <= 0.99999; }
+    static __device__ __forceinline__ double roulette_survivor(double w) { return w / 0.1; }
+    static __device__ __forceinline__ double zero_threshold() { return 1 - 0.99999; }
+    static __device__ __forceinline__ uint64_t qw(double w)
+    {
+        return __double2ull_rn(w * 4294967296.0);
     }
 };
 
@@ -93,19 +183,17 @@ struct MathFast {
 #define MC3D_TISSUE_AIR 0
 #define MC3D_TAB_STRIDE 3 /* float4 per tissue in the optical table */
 
-/* fixed-point weight, 2^-32 resolution */
-static __device__ __forceinline__ uint64_t qw(float w)
-{
-    return __float2ull_rn(w * 4294967296.0f);
-}
+/* fixed-point weight of the FP32 policies, 2^-32 resolution */
+static __device__ __forceinline__ uint64_t qw(float w) { return FloatTable::qw(w); }
 
 /* src/mc3d_gpu.cu:53-63 */
-template <class M>
-static __device__ __forceinline__ int grid_coord(float x, float ux, float d, float rd)
+template <class M, class R = typename M::real>
+static __device__ __forceinline__ int grid_coord(R x, R ux, float d_, float rd_)
 {
-    int i = (int)floorf(M::div_r(x, d, rd));
-    i += (x == (float)(int)((unsigned)i + 1u) * d);
-    float bmin = (float)i * d;
+    const R d = d_, rd = rd_;
+    int i = (int)M::floor(M::div_r(x, d, rd));
+    i += (x == (R)(int)((unsigned)i + 1u) * d);
+    R bmin = (R)i * d;
     i = ((x > bmin) || ((x == bmin) && (ux >= 0))) ? i : i - 1;
     return i;
 }
@@ -114,9 +202,8 @@ static __device__ __forceinline__ int grid_coord(float x, float ux, float d, flo
  * With JUMP the lookup reads the packed map (tissue | safe distance << 8, one
  * 16-bit load), so the safe distance rides in bits 8-15 of the result (0 above
  * the surface, where the tissue is air). */
-template <bool JUMP = false>
-static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, int k, float z,
-                                                float uz)
+template <bool JUMP = false, class R = float>
+static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, int k, R z, R uz)
 {
     int ci = min(max(i, 0), g.nx - 1);
     int cj = min(max(j, 0), g.ny - 1);
@@ -134,19 +221,18 @@ static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, 
 /* src/mc3d_gpu.cu:29-49.  With r > 0 the box is the cube of voxels within
  * Chebyshev distance r of (i, j, k) instead of the voxel itself; axes, if given,
  * receives the snapped axes (bit 0 x, 1 y, 2 z). */
-template <class M>
-static __device__ __forceinline__ float intersection(const GeomDev &g, int i, int j, int k,
-                                                     float *x, float ux, float *y, float uy,
-                                                     float *z, float uz, int r = 0,
-                                                     int *axes = nullptr)
+template <class M, class R = typename M::real>
+static __device__ __forceinline__ R intersection(const GeomDev &g, int i, int j, int k, R *x, R ux,
+                                                 R *y, R uy, R *z, R uz, int r = 0,
+                                                 int *axes = nullptr)
 {
-    float border_x = (float)((ux >= 0) ? (int)((unsigned)i + 1u + r) : i - r) * g.dx;
-    float t_x = M::div(border_x - *x, ux);
-    float border_y = (float)((uy >= 0) ? (int)((unsigned)j + 1u + r) : j - r) * g.dy;
-    float t_y = M::div(border_y - *y, uy);
-    float border_z = (float)((uz >= 0) ? (int)((unsigned)k + 1u + r) : k - r) * g.dz;
-    float t_z = M::div(border_z - *z, uz);
-    float t = fminf(t_x, fminf(t_y, t_z));
+    R border_x = (R)((ux >= 0) ? (int)((unsigned)i + 1u + r) : i - r) * (R)g.dx;
+    R t_x = M::div(border_x - *x, ux);
+    R border_y = (R)((uy >= 0) ? (int)((unsigned)j + 1u + r) : j - r) * (R)g.dy;
+    R t_y = M::div(border_y - *y, uy);
+    R border_z = (R)((uz >= 0) ? (int)((unsigned)k + 1u + r) : k - r) * (R)g.dz;
+    R t_z = M::div(border_z - *z, uz);
+    R t = M::fmin(t_x, M::fmin(t_y, t_z));
     *x = (t == t_x) ? border_x : *x + ux * t;
     *y = (t == t_y) ? border_y : *y + uy * t;
     *z = (t == t_z) ? border_z : *z + uz * t;
@@ -155,19 +241,23 @@ static __device__ __forceinline__ float intersection(const GeomDev &g, int i, in
 }
 
 /* src/mc3d_gpu.cu:113-126 */
-static __device__ __forceinline__ bool mirror(float *x, float *ux, float length)
+template <class M, class R = typename M::real>
+static __device__ __forceinline__ bool mirror(R *x, R *ux, float length_)
 {
+    const R length = length_;
     bool refl = (*x >= length) || (*x <= 0);
     *x = (*x >= length) ? 2 * length - *x : *x;
-    *x = (*x <= 0) ? fabsf(*x) : *x;
+    *x = (*x <= 0) ? M::fabs(*x) : *x;
     *ux = refl ? -1 * (*ux) : *ux;
     return refl;
 }
 
-struct Photon {
-    float x, y, z, ux, uy, uz, W, s;
+template <class R>
+struct PhotonT {
+    R x, y, z, ux, uy, uz, W, s;
     int i, j, k, tissue;
 };
+using Photon = PhotonT<float>;
 
 /* Per-thread tallies live in shared memory, one column per thread, so that the
  * step loop keeps only the photon in registers.  They are touched when a photon
@@ -198,10 +288,10 @@ struct Acc {
  * crossings inside the cube, which in the reference only move the photon (no
  * Fresnel event, absorption or scattering; their four random numbers are drawn
  * and discarded), are merged into this one step. */
-template <class M, bool AMAP, bool JUMP = false>
+template <class M, bool AMAP, bool JUMP = false, class R = typename M::real>
 static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float4 *tab,
-                                                   Photon &p, uint64_t &rx, uint32_t ra,
-                                                   const Acc &acc, float *db_out,
+                                                   PhotonT<R> &p, uint64_t &rx, uint32_t ra,
+                                                   const Acc &acc, R *db_out,
                                                    uint32_t *fresnel_count,
                                                    unsigned long long *amap, bool *lat_mirror)
 {
@@ -209,28 +299,28 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
      * (1-g^2, 1-g, 2g, 1+g^2) -- each the float the reference computes per step */
     const int tis = JUMP ? (p.tissue & 0xff) : p.tissue;
     const float4 *tt = tab + MC3D_TAB_STRIDE * tis;
-    float ni = tt[0].w;
-    float nt = ni;
-    const float mu_t = tt[1].x;
-    const float rmu_t = tt[1].z;
+    R ni = M::n(tt);
+    R nt = ni;
+    const R mu_t = M::mu_t(tt);
+    const R rmu_t = M::rmu_t(tt);
 
-    float newx = p.x, newy = p.y, newz = p.z;
+    R newx = p.x, newy = p.y, newz = p.z;
     int axes = 0;
-    float db = intersection<M>(g, p.i, p.j, p.k, &newx, p.ux, &newy, p.uy, &newz, p.uz,
+    R db = intersection<M>(g, p.i, p.j, p.k, &newx, p.ux, &newy, p.uy, &newz, p.uz,
                                JUMP ? (p.tissue >> 8) : 0, JUMP ? &axes : nullptr);
 
     bool hit = db * mu_t <= p.s;
-    float ds = hit ? db * mu_t : p.s;
+    R ds = hit ? db * mu_t : p.s;
     newx = hit ? newx : p.x + M::div_r(p.ux * ds, mu_t, rmu_t);
     newy = hit ? newy : p.y + M::div_r(p.uy * ds, mu_t, rmu_t);
     newz = hit ? newz : p.z + M::div_r(p.uz * ds, mu_t, rmu_t);
-    float s = p.s - ds;
+    R s = p.s - ds;
 
     int nexti = grid_coord<M>(newx, p.ux, g.dx, g.rdx);
     int nextj = grid_coord<M>(newy, p.uy, g.dy, g.rdy);
     int nextk = grid_coord<M>(newz, p.uz, g.dz, g.rdz);
     int next_tissue = tissue_at<JUMP>(g, nexti, nextj, nextk, newz, p.uz);
-    nt = tab[MC3D_TAB_STRIDE * (JUMP ? (next_tissue & 0xff) : next_tissue)].w;
+    nt = M::n(tab + MC3D_TAB_STRIDE * (JUMP ? (next_tissue & 0xff) : next_tissue));
 
     /* The voxel on the near side of the crossed face, which the reference's face
      * logic compares with the next voxel: the photon's own voxel in a one-voxel
@@ -243,24 +333,24 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
         bk = nextk - ((ax & 4) ? ((p.uz >= 0) ? 1 : -1) : 0);
     }
 
-    float tr_ux = p.ux, tr_uy = p.uy, tr_uz = p.uz;
+    R tr_ux = p.ux, tr_uy = p.uy, tr_uz = p.uz;
     bool refl = false;
     if (ni != nt) { /* src/mc3d_gpu.cu:226-257 */
-        float cos_ai = (bi != nexti) ? p.ux : ((bj != nextj) ? p.uy : p.uz);
-        cos_ai = fabsf(cos_ai);
+        R cos_ai = (bi != nexti) ? p.ux : ((bj != nextj) ? p.uy : p.uz);
+        cos_ai = M::fabs(cos_ai);
         cos_ai = (cos_ai > 1) ? 1 : cos_ai;
-        float ai = M::acos(cos_ai);
-        float ni_nt = M::div(ni, nt);
-        float sin_ai = M::sin(ai);
-        float sin_at = ni_nt * sin_ai;
-        float cos_at = M::sqrt(1.0f - sin_at * sin_at);
-        float R1 = M::div(sin_ai * cos_at - cos_ai * sin_at, sin_ai * cos_at + cos_ai * sin_at);
-        float R2 = M::div(cos_ai * cos_at - sin_ai * sin_at, cos_ai * cos_at + sin_at * sin_at);
-        float R = 0.5 * R1 * R1 * (1.0f + R2 * R2);
-        R = (sin_at > 1) ? 1 : R;
-        R = (ni == nt) ? 0 : R;
-        float lat = ni_nt; /* scale of the transmitted lateral cosines */
-        if (M::kFast && fabsf(1.0f - sin_at * sin_at) < MC3D_NEAR_CRITICAL_F) {
+        R ai = M::acos(cos_ai);
+        R ni_nt = M::div(ni, nt);
+        R sin_ai = M::sin(ai);
+        R sin_at = ni_nt * sin_ai;
+        R cos_at = M::sqrt((R)1 - sin_at * sin_at);
+        R R1 = M::div(sin_ai * cos_at - cos_ai * sin_at, sin_ai * cos_at + cos_ai * sin_at);
+        R R2 = M::div(cos_ai * cos_at - sin_ai * sin_at, cos_ai * cos_at + sin_at * sin_at);
+        R Rf = 0.5 * R1 * R1 * ((R)1 + R2 * R2); /* 0.5 is a double literal there too */
+        Rf = (sin_at > 1) ? 1 : Rf;
+        Rf = (ni == nt) ? 0 : Rf;
+        R lat = ni_nt; /* scale of the transmitted lateral cosines */
+        if (M::kFast && M::fabs((R)1 - sin_at * sin_at) < MC3D_NEAR_CRITICAL_F) {
             /* Near the critical angle 1 - sin_at^2 cancels in float and R is steep:
              * the same formulas in FP64, sin_ai from cos_ai directly, and the
              * transmitted direction renormalised in FP64. */
@@ -271,7 +361,7 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
             const double ca = sqrt(fmax((1.0 - st) * (1.0 + st), 0.0));
             const double R1 = (si * ca - c * st) / (si * ca + c * st);
             const double R2 = (c * ca - si * st) / (c * ca + st * st);
-            R = (st >= 1.0) ? 1.0f : (float)(0.5 * R1 * R1 * (1.0 + R2 * R2));
+            Rf = (st >= 1.0) ? (R)1 : (R)(0.5 * R1 * R1 * (1.0 + R2 * R2));
             const bool xa = bi != nexti;
             const bool ya = !xa && bj != nextj;
             const bool za = !xa && !ya && bk != nextk;
@@ -280,28 +370,28 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
             const double az = za ? 0.0 : (double)p.uz;
             const double lat2 = rn * rn * (ax * ax + ay * ay + az * az);
             const double sc = 1.0 / sqrt(ca * ca + lat2);
-            cos_at = (float)(ca * sc);
-            lat = (float)(rn * sc);
+            cos_at = (R)(ca * sc);
+            lat = (R)(rn * sc);
         }
         float eps = mc3d_rand_co(&rx, ra);
-        refl = eps < R;
+        refl = eps < Rf;
         tr_ux = refl ? p.ux * ((bi == nexti) ? 1 : -1)
-                     : ((bi != nexti) ? copysignf(cos_at, p.ux * cos_at) : p.ux * lat);
+                     : ((bi != nexti) ? M::copysign(cos_at, p.ux * cos_at) : p.ux * lat);
         tr_uy = refl ? p.uy * ((bj == nextj) ? 1 : -1)
-                     : (((bj != nextj) && (bi == nexti)) ? copysignf(cos_at, p.uy * cos_at)
+                     : (((bj != nextj) && (bi == nexti)) ? M::copysign(cos_at, p.uy * cos_at)
                                                            : p.uy * lat);
         tr_uz = refl ? p.uz * ((bk == nextk) ? 1 : -1)
                      : (((bk != nextk) && (bj == nextj) && (bi == nexti))
-                            ? copysignf(cos_at, p.uz * cos_at)
+                            ? M::copysign(cos_at, p.uz * cos_at)
                             : p.uz * lat);
         (*fresnel_count)++;
     }
 
     /* absorption, src/mc3d_gpu.cu:262-263 */
-    float W = p.W;
-    float dW = (mu_t > 0) ? tt[1].y * W : 0;
-    float W_before = W;
-    W = W - dW * (float)(!hit);
+    R W = p.W;
+    R dW = (mu_t > 0) ? M::albedo_c(tt) * W : 0;
+    R W_before = W;
+    W = W - dW * (R)(!hit);
     if (AMAP && !hit && mu_t > 0) {
         /* absorption map, the reference's disabled tally (src/mc3d_gpu.cu:265-272):
          * the current voxel clamped into the grid, fixed-point weight removed.  A
@@ -310,23 +400,23 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
         int ai = min(max(JUMP ? nexti : p.i, 0), g.nx - 1);
         int aj = min(max(JUMP ? nextj : p.j, 0), g.ny - 1);
         int ak = min(max(JUMP ? nextk : p.k, 0), g.nz - 1);
-        uint64_t dq = qw(W_before) - qw(W);
+        uint64_t dq = M::qw(W_before) - M::qw(W);
         if (dq) atomicAdd(amap + ((int64_t)ak * g.ny + aj) * g.nx + ai, (unsigned long long)dq);
     }
 
     /* russian roulette, src/mc3d_gpu.cu:275-277 */
     float eps = mc3d_rand_co(&rx, ra);
-    bool roulette = (W <= MC3D_W_THRESHOLD_LE_F) && (!hit) && (mu_t != 0);
+    bool roulette = M::w_below_threshold(W) && (!hit) && (mu_t != 0);
     if (roulette) {
-        float newW = (eps < MC3D_SURVIVAL_LT_F) ? (float)((double)W / MC3D_SURVIVAL_CHANCE) : 0.0f;
+        R newW = (eps < MC3D_SURVIVAL_LT_F) ? M::roulette_survivor(W) : (R)0;
         /* absorbed weight is booked at the photon's end as Q(W0) - Q(W_end) - lost;
          * a roulette event moves its share from there to the roulette tallies */
-        if (newW == 0.0f) {
-            uint64_t k = qw(W);
+        if (newW == 0) {
+            uint64_t k = M::qw(W);
             acc[T_RR_KILLED] += k;
             acc[T_ABSORBED] -= k;
         } else {
-            uint64_t c = qw(newW) - qw(W);
+            uint64_t c = M::qw(newW) - M::qw(W);
             acc[T_RR_CREATED] += c;
             acc[T_ABSORBED] += c;
         }
@@ -334,32 +424,30 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     }
 
     /* Henyey-Greenstein, src/mc3d_gpu.cu:282-294 */
-    const float4 t2 = tt[2];
-    float costheta = M::div(t2.x, t2.y + t2.z * mc3d_rand_oc(&rx, ra));
-    costheta = tt[1].w * (t2.w - costheta * costheta);
-    float sintheta = M::sqrt(1 - costheta * costheta);
-    float phi_divpi = 2 * mc3d_rand_co(&rx, ra);
-    float cosphi, sinphi;
+    R costheta = M::template hg_cos<M>(tt, (R)mc3d_rand_oc(&rx, ra));
+    R sintheta = M::sqrt(1 - costheta * costheta);
+    R phi_divpi = 2 * (R)mc3d_rand_co(&rx, ra);
+    R cosphi, sinphi;
     M::sincospi(phi_divpi, &sinphi, &cosphi);
-    float invsqrt = M::rsqrt(1 - p.uz * p.uz);
-    bool steep = !(fabsf(p.uz) <= MC3D_UZ_THRESH_LE_F);
-    float sc_ux = !steep ? sintheta * (p.ux * p.uz * cosphi - p.uy * sinphi) * invsqrt +
-                               p.ux * costheta
-                         : sintheta * cosphi;
-    float sc_uy = !steep ? sintheta * (p.uy * p.uz * cosphi + p.ux * sinphi) * invsqrt +
-                               p.uy * costheta
-                         : sintheta * sinphi;
-    float sc_uz = !steep ? -1 * M::sqrt(1 - p.uz * p.uz) * sintheta * cosphi + p.uz * costheta
-                         : copysignf(costheta, costheta * p.uz);
+    R invsqrt = M::rsqrt(1 - p.uz * p.uz);
+    bool steep = !M::uz_within(M::fabs(p.uz));
+    R sc_ux = !steep ? sintheta * (p.ux * p.uz * cosphi - p.uy * sinphi) * invsqrt +
+                           p.ux * costheta
+                     : sintheta * cosphi;
+    R sc_uy = !steep ? sintheta * (p.uy * p.uz * cosphi + p.ux * sinphi) * invsqrt +
+                           p.uy * costheta
+                     : sintheta * sinphi;
+    R sc_uz = !steep ? -1 * M::sqrt(1 - p.uz * p.uz) * sintheta * cosphi + p.uz * costheta
+                     : M::copysign(costheta, costheta * p.uz);
 
-    float nux = (!hit) ? sc_ux : tr_ux;
-    float nuy = (!hit) ? sc_uy : tr_uy;
-    float nuz = (!hit) ? sc_uz : tr_uz;
-    const float zero_thresh = (float)(1 - MC3D_UZ_THRESH);
-    nux = (fabsf(nux) < zero_thresh) ? 0 : nux;
-    nuy = (fabsf(nuy) < zero_thresh) ? 0 : nuy;
-    nuz = (fabsf(nuz) < zero_thresh) ? 0 : nuz;
-    float norm = M::rsqrt(nux * nux + nuy * nuy + nuz * nuz);
+    R nux = (!hit) ? sc_ux : tr_ux;
+    R nuy = (!hit) ? sc_uy : tr_uy;
+    R nuz = (!hit) ? sc_uz : tr_uz;
+    const R zero_thresh = M::zero_threshold();
+    nux = (M::fabs(nux) < zero_thresh) ? 0 : nux;
+    nuy = (M::fabs(nuy) < zero_thresh) ? 0 : nuy;
+    nuz = (M::fabs(nuz) < zero_thresh) ? 0 : nuz;
+    R norm = M::rsqrt(nux * nux + nuy * nuy + nuz * nuz);
     nux *= norm;
     nuy *= norm;
     nuz *= norm;
@@ -370,7 +458,7 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     p.uz = !freeze ? nuz : p.uz;
 
     float e2 = mc3d_rand_oc(&rx, ra);
-    float newS = (W > 0) ? -M::log(e2) : 0;
+    R newS = (W > 0) ? -M::log((R)e2) : 0;
     p.s = (freeze || hit) ? s : newS;
     p.W = W;
 
@@ -382,7 +470,7 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
      * lateral faces both mirrors are no-ops, which one rarely taken branch tests */
     bool fres_refl = refl;
     if (!(p.x > 0 && p.x < g.Lx && p.y > 0 && p.y < g.Ly))
-        refl = refl || mirror(&p.x, &p.ux, g.Lx) || mirror(&p.y, &p.uy, g.Ly);
+        refl = refl || mirror<M>(&p.x, &p.ux, g.Lx) || mirror<M>(&p.y, &p.uy, g.Ly);
     *lat_mirror = refl && !fres_refl;
 
     bool keep = (hit && refl) || freeze;
@@ -407,8 +495,8 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
 
 /* i, j, k and tissue from the position, as at the start of every launch of
  * photontrack_step (src/mc3d_gpu.cu:168-171). */
-template <class M, bool JUMP = false>
-static __device__ __forceinline__ void derive_cell(const GeomDev &g, Photon &p)
+template <class M, bool JUMP = false, class R = typename M::real>
+static __device__ __forceinline__ void derive_cell(const GeomDev &g, PhotonT<R> &p)
 {
     p.i = grid_coord<M>(p.x, p.ux, g.dx, g.rdx);
     p.j = grid_coord<M>(p.y, p.uy, g.dy, g.rdy);
@@ -420,18 +508,20 @@ static __device__ __forceinline__ void derive_cell(const GeomDev &g, Photon &p)
  * every axis: strictly inside, or on the lower face moving up, or on the upper face
  * moving down.  Then re-deriving the cell and tissue at a launch boundary changes
  * nothing (above the surface the air rule would apply, which needs z > 0 here). */
-static __device__ __forceinline__ bool cell_consistent(const GeomDev &g, const Photon &p)
+template <class R>
+static __device__ __forceinline__ bool cell_consistent(const GeomDev &g, const PhotonT<R> &p)
 {
-    const float xl = (float)p.i * g.dx, xh = (float)(p.i + 1) * g.dx;
-    const float yl = (float)p.j * g.dy, yh = (float)(p.j + 1) * g.dy;
-    const float zl = (float)p.k * g.dz, zh = (float)(p.k + 1) * g.dz;
+    const R xl = (R)p.i * (R)g.dx, xh = (R)(p.i + 1) * (R)g.dx;
+    const R yl = (R)p.j * (R)g.dy, yh = (R)(p.j + 1) * (R)g.dy;
+    const R zl = (R)p.k * (R)g.dz, zh = (R)(p.k + 1) * (R)g.dz;
     const bool ox = (p.x > xl && p.x < xh) || (p.x == xl && p.ux >= 0) || (p.x == xh && p.ux < 0);
     const bool oy = (p.y > yl && p.y < yh) || (p.y == yl && p.uy >= 0) || (p.y == yh && p.uy < 0);
     const bool oz = (p.z > zl && p.z < zh) || (p.z == zl && p.uz >= 0) || (p.z == zh && p.uz < 0);
     return ox && oy && oz && p.z > 0;
 }
 
-static __device__ __forceinline__ bool finite_state(const Photon &p)
+template <class R>
+static __device__ __forceinline__ bool finite_state(const PhotonT<R> &p)
 {
     return isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(p.s) &&
            isfinite(p.ux) && isfinite(p.uy) && isfinite(p.uz);
@@ -439,7 +529,8 @@ static __device__ __forceinline__ bool finite_state(const Photon &p)
 
 /* The NaN/Inf/db==0 quickfix run after each 45-step launch (src/mc3d_gpu.cu:343-353).
  * Returns true (and zeroes the photon) when it fires. */
-static __device__ __forceinline__ bool quickfix(Photon &p, float db)
+template <class R>
+static __device__ __forceinline__ bool quickfix(PhotonT<R> &p, R db)
 {
     if (!finite_state(p) || db == 0) {
         p.x = 0; p.y = 0; p.z = 0;
@@ -453,14 +544,13 @@ static __device__ __forceinline__ bool quickfix(Photon &p, float db)
 /* The steps a frozen slot keeps executing until the end of its 45-step launch.
  * They change nothing but the mirror (which flips u while the photon sits on a
  * lateral face) and the boundary distance the quickfix looks at. */
-template <class M>
-static __device__ __forceinline__ float masked_steps(const GeomDev &g, Photon &p, int masked,
-                                                     float db)
+template <class M, class R = typename M::real>
+static __device__ __forceinline__ R masked_steps(const GeomDev &g, PhotonT<R> &p, int masked, R db)
 {
     for (int t = 0; t < masked; t++) {
-        float nx_ = p.x, ny_ = p.y, nz_ = p.z;
+        R nx_ = p.x, ny_ = p.y, nz_ = p.z;
         db = intersection<M>(g, p.i, p.j, p.k, &nx_, p.ux, &ny_, p.uy, &nz_, p.uz);
-        if (!mirror(&p.x, &p.ux, g.Lx)) mirror(&p.y, &p.uy, g.Ly);
+        if (!mirror<M>(&p.x, &p.ux, g.Lx)) mirror<M>(&p.y, &p.uy, g.Ly);
     }
     return db;
 }
@@ -519,6 +609,7 @@ static __device__ __forceinline__ uint64_t stream_seed(const KernelParams &P, co
 template <class M, bool AMAP, bool JUMP = false, bool ONE_GEOM = false>
 __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
 {
+    using R = typename M::real;
     /* dynamic shared memory: the optical tables, then (several geometries) the
      * geometry descriptors, read from there instead of being held per thread */
     extern __shared__ float4 sh_tab[];
@@ -537,7 +628,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
     int64_t left = 0, local = 0;
     uint64_t rx = 0;
     uint32_t ra = 1;
-    Photon p;
+    PhotonT<R> p;
     bool alive = false;
     int chunk = 0;
     uint32_t psteps = 0;
@@ -567,21 +658,21 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
             const GeomDev &g = ONE_GEOM ? P.geom0 : *gp;
             /* photontrack_reinitialize, src/mc3d_gpu.cu:74-111 */
             if (P.jobs[job].beam == 0) {
-                p.x = g.Lx * mc3d_rand_co(&rx, ra);
-                p.y = g.Ly * mc3d_rand_co(&rx, ra);
+                p.x = (R)g.Lx * (R)mc3d_rand_co(&rx, ra);
+                p.y = (R)g.Ly * (R)mc3d_rand_co(&rx, ra);
             } else {
-                p.x = g.Lx / 2;
-                p.y = g.Ly / 2;
+                p.x = (R)g.Lx / 2;
+                p.y = (R)g.Ly / 2;
             }
             p.z = 0;
             p.ux = 0; p.uy = 0; p.uz = 1;
             /* specular reflection from air into tissue type 1 (src/mc3d_gpu.cu:67-70, 500) */
-            const float n0 = tab[MC3D_TAB_STRIDE * MC3D_TISSUE_AIR].w, n1 = tab[MC3D_TAB_STRIDE].w;
-            float rsp = M::div(n0 - n1, n0 + n1);
+            const R n0 = M::n(tab + MC3D_TAB_STRIDE * MC3D_TISSUE_AIR), n1 = M::n(tab + MC3D_TAB_STRIDE);
+            R rsp = M::div(n0 - n1, n0 + n1);
             rsp = rsp * rsp;
-            p.W = 1.0f - rsp;
-            qw0 = qw(p.W);
-            p.s = -M::log(mc3d_rand_oc(&rx, ra));
+            p.W = (R)1 - rsp;
+            qw0 = M::qw(p.W);
+            p.s = -M::log((R)mc3d_rand_oc(&rx, ra));
             derive_cell<M, JUMP>(g, p);
             chunk = 0;
             psteps = 0;
@@ -591,7 +682,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
         }
 
         const GeomDev &g = ONE_GEOM ? P.geom0 : *gp;
-        float db;
+        R db;
         bool lat_mirror;
         bool froze;
         froze = photon_step<M, AMAP, JUMP>(g, tab, p, rx, ra, acc, &db, &fresnel, amap,
@@ -607,14 +698,14 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
              * step's boundary distance again: no need to replay them. */
             if (lat_mirror || !(p.x > 0 && p.x < g.Lx && p.y > 0 && p.y < g.Ly))
                 db = masked_steps<M>(g, p, MC3D_NUM_PHOTON_STEPS - chunk, db);
-            float w_before = p.W;
-            if (quickfix(p, db)) { acc[T_QUICKFIX]++; lost = qw(w_before); }
+            R w_before = p.W;
+            if (quickfix(p, db)) { acc[T_QUICKFIX]++; lost = M::qw(w_before); }
             done = true;
         } else if (chunk == MC3D_NUM_PHOTON_STEPS) {
-            float w_before = p.W;
+            R w_before = p.W;
             if (quickfix(p, db)) {
                 acc[T_QUICKFIX]++;
-                lost = qw(w_before);
+                lost = M::qw(w_before);
                 done = true;
             } else {
                 /* fast math: re-derive only where the stored cell breaks the face rule
@@ -624,7 +715,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
             }
         }
         if (!done && (int64_t)psteps >= max_steps) {
-            lost = qw(p.W);
+            lost = M::qw(p.W);
             p.W = 0;
             acc[T_CAPPED]++;
             done = true;
@@ -635,14 +726,14 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
             int ix = grid_coord<M>(p.x, p.ux, g.dx, g.rdx);
             int iy = grid_coord<M>(p.y, p.uy, g.dy, g.rdy);
             bool inside = (ix >= 0) && (iy >= 0) && (ix < g.nx) && (iy < g.ny);
-            uint64_t q = qw(p.W);
+            uint64_t q = M::qw(p.W);
             int64_t bin = jb.bin_offset + (int64_t)iy * g.nx + ix;
             int slot;
             if (p.z <= 0) {
                 slot = inside ? T_R_IN : T_R_OUT;
                 if (inside && q) {
                     atomicAdd(P.drs + bin, (unsigned long long)q);
-                    atomicAdd(P.drs_sq + bin, (unsigned long long)qw(p.W * p.W));
+                    atomicAdd(P.drs_sq + bin, (unsigned long long)M::qw(p.W * p.W));
                 }
             } else {
                 slot = inside ? T_T_IN : T_T_OUT;
@@ -660,9 +751,9 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
                 int64_t kphot = nstream - left - 1;
                 int64_t pid = jb.photon_base + local + kphot * jb.streams;
                 PhotonRecord r;
-                r.x = p.x; r.y = p.y; r.z = p.z;
-                r.ux = p.ux; r.uy = p.uy; r.uz = p.uz;
-                r.W = p.W; r.s = p.s;
+                r.x = (float)p.x; r.y = (float)p.y; r.z = (float)p.z;
+                r.ux = (float)p.ux; r.uy = (float)p.uy; r.uz = (float)p.uz;
+                r.W = (float)p.W; r.s = (float)p.s;
                 r.steps = psteps;
                 r.tissue = (uint32_t)(p.tissue & 0xff);
                 r.rng = rx;
