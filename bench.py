@@ -502,7 +502,8 @@ def run_batched(args):
         return sum(ts) / len(ts), res
 
     with ClockSampler(dev) as clocks:
-        plan = m.Plan(w.geoms, w.props, w.jobs, math=args.math, device=dev, steps=args.step_mode)
+        plan = m.Plan(w.geoms, w.props, w.jobs, math=args.math, device=dev, steps=args.step_mode,
+                      use_graph=True)
         t_batch, res = timed(plan, args.steps, args.warmup)
         plan.close()
         photons = sum(r.photons for r in res)
@@ -526,7 +527,9 @@ def run_batched(args):
             "vs_baseline": None, "dtype": "f64+u64" if args.math == "f64" else "f32+u64", "data": "synthetic (seeded)",
             "config": {"workload": w.name, "jobs": len(w.jobs), "photons_per_step": photons,
                        "math": args.math, "step_mode": args.step_mode,
-                       "photon_scale": args.photon_scale},
+                       "photon_scale": args.photon_scale,
+                       "batched": "one persistent launch over all jobs, replayed from a CUDA "
+                                  "graph (tally clear + kernel)"},
             "steps_per_s": steps / t_batch, "plain": plain, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
 
