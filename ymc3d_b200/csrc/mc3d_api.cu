@@ -64,10 +64,15 @@ void make_seed_consts(uint32_t begin, mc3d_seed_consts *c)
     unsigned __int128 r1 = (((unsigned __int128)1) << 64) % m;
     c->r2 = (uint64_t)((r1 * r1) % m);
     c->begin = begin;
-    uint64_t p = (uint64_t)(((unsigned __int128)begin * begin) % m); /* one attempt = 2 draws */
-    for (int k = 0; k < MC3D_JUMP_BITS; k++) {
-        c->jump[k] = (uint64_t)(((unsigned __int128)p * r1) % m); /* Montgomery form */
-        p = (uint64_t)(((unsigned __int128)p * p) % m);
+    /* base = a^(2 16^w): one attempt is two draws of the seeding generator */
+    uint64_t base = (uint64_t)(((unsigned __int128)begin * begin) % m);
+    for (int w = 0; w < MC3D_JUMP_WINDOWS; w++) {
+        uint64_t p = base;
+        for (int d = 1; d <= 15; d++) {
+            c->jump[w][d - 1] = (uint64_t)(((unsigned __int128)p * r1) % m); /* Montgomery form */
+            p = (uint64_t)(((unsigned __int128)p * base) % m);
+        }
+        base = p; /* base^16 */
     }
 }
 
@@ -530,6 +535,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     P.photon_log = p->d_log;
     P.amap = p->d_amap;
     P.num_multipliers = table_len;
+    P.mult_magic = UINT64_MAX / (uint64_t)(table_len - 1);
     P.total_streams = stream_base;
     P.max_steps = opt.max_steps > 0 ? std::min<int64_t>(opt.max_steps, INT32_MAX) : (1 << 24);
     P.njobs = njobs;
@@ -700,6 +706,7 @@ int mc3d_stream_seeds(const mc3d_job *job, const uint32_t *table, int64_t table_
         P.jobs = d_job;
         P.multipliers = d_mult;
         P.num_multipliers = table_len;
+        P.mult_magic = UINT64_MAX / (uint64_t)(table_len - 1);
         P.rejections = d_rej;
         P.njobs = 1;
         P.seed = sc;

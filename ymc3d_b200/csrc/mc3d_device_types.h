@@ -81,6 +81,7 @@ struct KernelParams {
     const int *cancel;
     PhotonRecord *photon_log;
     int64_t num_multipliers;
+    uint64_t mult_magic;      /* floor((2^64 - 1) / (num_multipliers - 1)), see stream_multiplier */
     int64_t total_streams;
     int64_t max_steps;
     int32_t njobs;

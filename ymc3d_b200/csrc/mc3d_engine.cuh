@@ -572,6 +572,19 @@ static __device__ __forceinline__ void acc_flush(const Acc &a, unsigned long lon
     }
 }
 
+/* Multiplier of job-local stream `local`: table line 1 + local mod (L - 1).  The
+ * remainder by Barrett reduction with magic = floor((2^64 - 1) / (L - 1)): the
+ * quotient estimate is at most one short, so one correction gives the remainder
+ * (local < 2^63). */
+static __device__ __forceinline__ uint32_t stream_multiplier(const KernelParams &P, int64_t local)
+{
+    const uint64_t d = (uint64_t)(P.num_multipliers - 1);
+    const uint64_t q = __umul64hi((uint64_t)local, P.mult_magic);
+    uint64_t r = (uint64_t)local - q * d;
+    r = (r >= d) ? r - d : r;
+    return P.multipliers[1 + r];
+}
+
 /* job owning global stream index gs (binary search over the stream prefix) */
 static __device__ __forceinline__ int find_job(const JobDev *jobs, int njobs, int64_t gs)
 {
@@ -640,18 +653,21 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
     for (;;) {
         if (!alive) {
             if (left == 0) {
-                if (job >= 0) acc_flush(acc, P.totals + (int64_t)job * MC3D_NUM_TOTALS);
                 if (P.cancel && *((volatile const int *)P.cancel)) break;
                 int64_t gs = (int64_t)atomicAdd((unsigned long long *)P.work_counter, 1ull);
                 if (gs >= P.total_streams) break;
-                job = find_job(P.jobs, P.njobs, gs);
+                const int next_job = find_job(P.jobs, P.njobs, gs);
+                /* the per-thread tallies are the job's: flushed when the job changes */
+                if (job >= 0 && next_job != job)
+                    acc_flush(acc, P.totals + (int64_t)job * MC3D_NUM_TOTALS);
+                job = next_job;
                 const JobDev &jb = P.jobs[job];
                 gp = sh_geom + jb.geom;
                 tab = sh_tab + jb.props_offset;
                 if (AMAP) amap = P.amap + jb.amap_offset;
                 local = gs - jb.stream_base + jb.stream_first;
                 left = jb.per_stream + (local < jb.remainder ? 1 : 0);
-                ra = P.multipliers[1 + (local % (P.num_multipliers - 1))];
+                ra = stream_multiplier(P, local);
                 rx = stream_seed(P, jb, local, ra);
                 if (left == 0) continue;
             }

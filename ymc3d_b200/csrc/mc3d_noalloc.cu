@@ -248,6 +248,7 @@ extern "C" int mc3d_run_noalloc(const mc3d_geom *geom, const mc3d_props *props,
     P.totals = (unsigned long long *)totals;
     P.work_counter = words;
     P.num_multipliers = table_len;
+    P.mult_magic = UINT64_MAX / (uint64_t)(table_len - 1);
     P.total_streams = count;
     P.max_steps = 1 << 24;
     P.njobs = 1;

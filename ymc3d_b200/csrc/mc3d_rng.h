@@ -87,16 +87,18 @@ MC3D_RNG_FN uint64_t mc3d_mont_mul(uint64_t a, uint64_t b, uint64_t m, uint64_t 
 }
 
 /* Everything a stream needs to compute its seed: the seeding modulus, its
- * Montgomery constants and (a^(2^(k+1)) R mod m) for k = 0..MC3D_JUMP_BITS-1,
- * i.e. the jump by 2^k seeding attempts (two draws each). */
+ * Montgomery constants and, for 4-bit windows w = 0..MC3D_JUMP_WINDOWS-1 and digits
+ * d = 1..15, (a^(2 d 16^w) R mod m): the jump by d 16^w seeding attempts (two
+ * draws each).  A jump by t < 2^40 attempts is at most ten products. */
 #define MC3D_JUMP_BITS 40
+#define MC3D_JUMP_WINDOWS (MC3D_JUMP_BITS / 4)
 typedef struct {
     uint64_t m;      /* begin * 2^32 - 1 */
     uint64_t ninv;   /* -m^-1 mod 2^64 */
     uint64_t r2;     /* R^2 mod m */
     uint32_t begin;
     uint32_t pad;
-    uint64_t jump[MC3D_JUMP_BITS];
+    uint64_t jump[MC3D_JUMP_WINDOWS][15];
 } mc3d_seed_consts;
 
 /* packed state validity, gpumcml_rng/gpumcml_rng.cu:100 */
@@ -128,8 +130,9 @@ MC3D_RNG_FN uint64_t mc3d_seed_attempt(uint64_t xs, uint32_t begin, uint32_t for
 MC3D_RNG_FN uint64_t mc3d_seed_jump(const mc3d_seed_consts *c, uint64_t xinit, uint64_t t)
 {
     uint64_t xm = mc3d_mont_mul(xinit, c->r2, c->m, c->ninv); /* to Montgomery form */
-    for (int k = 0; k < MC3D_JUMP_BITS && t != 0; k++, t >>= 1) {
-        if (t & 1u) xm = mc3d_mont_mul(xm, c->jump[k], c->m, c->ninv);
+    for (int w = 0; w < MC3D_JUMP_WINDOWS && t != 0; w++, t >>= 4) {
+        const unsigned d = (unsigned)(t & 15u);
+        if (d) xm = mc3d_mont_mul(xm, c->jump[w][d - 1], c->m, c->ninv);
     }
     return mc3d_mont_mul(xm, 1u, c->m, c->ninv); /* out of Montgomery form */
 }
