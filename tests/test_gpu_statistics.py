@@ -155,3 +155,14 @@ def test_cancel_flag_stops_and_keeps_partial_tallies_consistent(table):
     part = e.value.results[0]
     assert part.photons < 500_000
     assert part.conservation_residual() == 0
+
+
+def test_skin_model_runs(table):
+    """the MATLAB example model, restated in workloads.py, through the engine:
+    exact conservation and reflectance from every layer's surface bins"""
+    from ymc3d_b200 import workloads as W
+    g = W.skin_geometry()
+    p = W.skin_optprops(600.0, lambda oxy, lam: 2e4 * (1 + oxy))
+    r = m.run([g], [p], [m.Job(0, 0, 200_000, 5, "uniform")], table=table)[0]
+    assert r.photons == 200_000 and residual(r.totals) == 0
+    assert 0 < r.totals["r_in"] < r.totals["w_launched"]

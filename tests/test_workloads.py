@@ -68,10 +68,21 @@ def test_skin_model_matches_the_matlab_recipe():
     assert (nx, ny, nz) == (50, 50, 85)
     col = g.tissue[:, 0, 0]
     # epidermis 0.1 mm = 5 voxels, papillary 10 % of 1.5 mm = 7, reticular 67
-    assert np.all(col[:5] == 1) and np.all(col[5:12] == 2) and np.all(col[12:79] == 3)
-    assert np.all(col[79:] == 4)
-    assert (g.tissue == 5).sum() > 0 and np.all(g.tissue[:, 0, :] == g.tissue[:, -1, :])
-    p = W.skin_optprops(600.0, lambda oxy, lam: 1e4 * (1 + oxy))
-    assert p.num_tissue_types == 6
+    assert np.all(col[:5] == W.SKIN_EPIDERMIS) and np.all(col[5:12] == W.SKIN_PAPILLARY)
+    assert np.all(col[12:79] == W.SKIN_RETICULAR) and np.all(col[79:] == W.SKIN_SUBCUTIS)
+    vessel = g.tissue == W.SKIN_VESSEL
+    assert vessel.sum() > 0 and np.all(g.tissue[:, 0, :] == g.tissue[:, -1, :])
+    # voxel (i, k) 1-based is in the vessel when (i dx - 0.5)^2 + (k dx - 0.25)^2 <= 0.06^2
+    k, i = np.nonzero(vessel[:, 0, :])
+    assert np.all(((i + 1) * 0.02 - 0.5) ** 2 + ((k + 1) * 0.02 - 0.25) ** 2 <= 0.06 ** 2 + 1e-12)
+    blood = lambda oxy, lam: 1e4 * (1 + oxy)  # noqa: E731
+    rows = W.skin_optprops_rows(600.0, blood)
+    assert len(rows) == 3
+    mel = (600 / 694) ** -3.46
+    assert abs(rows[0][0] - (227 * mel + 0.002 * 1.5e4 + 0.988 * 25) * 0.01) < 1e-9
+    assert abs(rows[1][0] - (0.01 * 1.5e4 + 0.99 * 25) * 0.01) < 1e-9
+    assert abs(rows[2][0] - (0.01 * 1.8e4 + 0.99 * 25) * 0.01) < 1e-9
+    p = W.skin_optprops(600.0, blood)
+    assert p.num_tissue_types == 7  # air + six tissues, the grid's largest index is 6
     assert abs(p.g[1] - (0.62 + 600 * 29e-5)) < 1e-6
-    assert p.mua[5] > p.mua[3] > 0 and np.all(p.n[1:] == np.float32(1.4))
+    assert p.mua[6] > p.mua[3] > 0 and np.all(p.n[1:] == np.float32(1.4))

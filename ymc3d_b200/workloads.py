@@ -79,47 +79,62 @@ def read_drs_file(path: str | os.PathLike) -> tuple[np.ndarray, float, float]:
 
 
 # ------------------------------------------------------------------ skin model
+SKIN_EPIDERMIS, SKIN_PAPILLARY, SKIN_RETICULAR, SKIN_SUBCUTIS, SKIN_MOLE, SKIN_VESSEL = 1, 2, 3, 4, 5, 6
+
+
 def skin_geometry(dx: float = 0.02, length_xy: float = 1.0, length_z: float = 1.7,
                   epi: float = 0.1, dermis: float = 1.5, papillary_frac: float = 0.1,
                   vessel_radius: float = 0.06, vessel_depth: float = 0.25) -> Geometry:
     """The example model of matlab/geometry/prepare_geometry.m:2-55: epidermis,
     papillary and reticular dermis, subcutis, and a blood vessel along y at half
-    the width.  Tissue indices 1..5 (file values 0..4 there, vessel 5 -> 6 here
-    is folded to index 5: epidermis 1, papillary 2, reticular 3, subcutis 4,
-    vessel 5).  As in the script, voxel n (1-based) is tested at n * dx."""
+    the width.  The script writes file values 0 (epidermis) .. 5 (vessel, 4 being
+    an unused mole); the reader adds one (src/mc3d_io.cu:155-163), so the grid
+    holds SKIN_EPIDERMIS .. SKIN_VESSEL = 1 .. 6.  As in the script, voxel n
+    (1-based) is tested for the vessel at n * dx."""
     nx = ny = int(round(length_xy / dx))
     nz = int(round(length_z / dx))
     epi_vox = int(np.floor(epi / dx))
     pap_vox = epi_vox + int(np.floor(papillary_frac * dermis / dx))
     ret_vox = pap_vox + int(np.floor((1 - papillary_frac) * dermis / dx))
     k = np.arange(nz)
-    layer = np.where(k < epi_vox, 1, np.where(k < pap_vox, 2, np.where(k < ret_vox, 3, 4)))
+    layer = np.where(k < epi_vox, SKIN_EPIDERMIS,
+                     np.where(k < pap_vox, SKIN_PAPILLARY,
+                              np.where(k < ret_vox, SKIN_RETICULAR, SKIN_SUBCUTIS)))
     t = np.broadcast_to(layer.astype(np.uint8)[:, None, None], (nz, ny, nx)).copy()
     xi = (np.arange(nx) + 1) * dx
     zk = (np.arange(nz) + 1) * dx
     vessel = ((xi[None, :] - length_xy / 2) ** 2 + (zk[:, None] - vessel_depth) ** 2
               <= vessel_radius ** 2)
-    t[np.broadcast_to(vessel[:, None, :], t.shape)] = 5
+    t[np.broadcast_to(vessel[:, None, :], t.shape)] = SKIN_VESSEL
     return Geometry(t, dx, dx, dx)
 
 
-def skin_optprops(lam: float, mua_blood) -> OpticalProps:
-    """Optical properties of prepare_optprops.m:29-51 at wavelength `lam` (nm), in
-    1/mm, for skin_geometry's tissues.  mua_blood(oxygenation, lam) is the whole-
-    blood absorption in 1/m; the reference reads it from muab.mat, which it does
-    not distribute, so the caller supplies it.  The subcutis and vessel rows are
-    not in the script (its example is explicitly incomplete); they take the
-    reticular dermis values and whole blood at oxygenation 0.8, g 0.98."""
+def skin_optprops_rows(lam: float, mua_blood) -> list[tuple[float, float, float, float]]:
+    """The three (mua, mus, g, n) rows of prepare_optprops.m:29-51 at wavelength
+    `lam` (nm), in 1/mm: epidermis, papillary dermis, reticular dermis.
+    mua_blood(oxygenation, lam) is the whole-blood absorption in 1/m; the script
+    interpolates it from muab.mat, which the reference does not distribute, so the
+    caller supplies it."""
     melanin = (lam / 694.0) ** -3.46
     musr = 100 * (18.780 * (lam / 500.0) ** -0.22 + 17.6 * (lam / 500.0) ** -4)
     g = 0.62 + lam * 29e-5
     mus = musr / (1 - g) * 0.01
-    rows = [((227 * melanin + 0.002 * mua_blood(0.5, lam) + (1 - 0.01 - 0.002) * 25) * 0.01,
+    return [((227 * melanin + 0.002 * mua_blood(0.5, lam) + (1 - 0.01 - 0.002) * 25) * 0.01,
              mus, g, 1.4),
             ((0.01 * mua_blood(0.5, lam) + (1 - 0.01) * 25) * 0.01, mus, g, 1.4),
-            ((0.01 * mua_blood(0.8, lam) + (1 - 0.01) * 25) * 0.01, mus, g, 1.4),
-            ((0.01 * mua_blood(0.8, lam) + (1 - 0.01) * 25) * 0.01, mus, g, 1.4),
-            (mua_blood(0.8, lam) * 0.01, mus, 0.98, 1.4)]
+            ((0.01 * mua_blood(0.8, lam) + (1 - 0.01) * 25) * 0.01, mus, g, 1.4)]
+
+
+def skin_optprops(lam: float, mua_blood) -> OpticalProps:
+    """An optical set for every tissue of skin_geometry.  Rows 1-3 are the
+    script's (skin_optprops_rows).  The script stops there ("a very simple
+    example"), though its geometry also holds subcutis, mole and vessel voxels;
+    rows 4-6 are this module's stand-ins so that the model runs: subcutis and
+    mole as reticular dermis, the vessel as whole blood at oxygenation 0.8
+    (mua_blood(0.8) in 1/mm) with the dermis scattering and g 0.98."""
+    rows = skin_optprops_rows(lam, mua_blood)
+    ret = rows[2]
+    rows += [ret, ret, (mua_blood(0.8, lam) * 0.01, ret[1], 0.98, 1.4)]
     return OpticalProps.from_tissues(rows)
 
 
