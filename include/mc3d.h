@@ -59,7 +59,8 @@ enum mc3d_math { MC3D_MATH_FAST = 0, MC3D_MATH_EXACT = 1, MC3D_MATH_F64 = 2 };
  * map, built when the plan is created); each replaced crossing would only have
  * moved the photon.  VOXEL steps at every voxel face, as the reference does
  * (src/mc3d_gpu.cu:181-339).  Both are the reference's physics; the step counts
- * in mc3d_totals differ.  Exact math always steps at every face. */
+ * in mc3d_totals differ.  Exact math always steps at every face, and so does
+ * a launch with a geometry of nx * ny * (nz + 63) >= 2^32 voxels. */
 enum mc3d_steps { MC3D_STEPS_MERGED = 0, MC3D_STEPS_VOXEL = 1 };
 
 /* Voxel geometry (geometry_t, src/mc3d_types.h:38-43), tissue indices as uint8

@@ -369,6 +369,11 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     std::vector<GeomDev> gh(ngeoms);
     p->d_grids.assign(ngeoms, nullptr);
     p->jump = p->math == MC3D_MATH_FAST && opt.steps != MC3D_STEPS_VOXEL;
+    /* the merged kernel indexes its cell map in 32 bits: larger grids step per face */
+    for (int i = 0; i < ngeoms; i++)
+        if ((uint64_t)geoms[i].nx * geoms[i].ny * ((uint64_t)geoms[i].nz + MC3D_SAFE_CAP) >=
+            (1ull << 32))
+            p->jump = false;
     size_t max_map = 0; /* largest safe-distance map, nz + MC3D_SAFE_CAP slices */
     for (int i = 0; i < ngeoms; i++) {
         const mc3d_geom &g = geoms[i];

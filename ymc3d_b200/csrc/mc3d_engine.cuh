@@ -211,7 +211,9 @@ static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, 
     int t;
     if (JUMP) {
         const int rk = min(max(k, 0), g.nz - 1 + MC3D_SAFE_CAP);
-        t = __ldg(g.cells + ((int64_t)rk * g.ny + cj) * g.nx + ci);
+        /* 32-bit index: plans take merged steps only for maps below 2^32 cells */
+        t = __ldg(g.cells + (((uint32_t)rk * (uint32_t)g.ny + (uint32_t)cj) * (uint32_t)g.nx +
+                             (uint32_t)ci));
     } else {
         t = __ldg(g.tissue + ((int64_t)ck * g.ny + cj) * g.nx + ci);
     }
