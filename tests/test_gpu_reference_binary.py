@@ -75,3 +75,18 @@ def test_homogeneous_vs_reference(tmp_path, table):
               [m.Job(0, 0, 2_000_000, 777, "uniform")], table=table)[0]
     chi2, dof, pv = compare(r, R, fin, 4)
     assert dof >= 32 and pv > 1e-4, (chi2, dof, pv)
+
+
+def test_headline_geometry_vs_reference(tmp_path, table):
+    """the benchmark's own geometry (256x256x128 at 0.02 mm, layers and vessel):
+    the reference at 4e6 photons against the engine's default fast path"""
+    g = layered_vessel_geometry(256, 256, 128, 0.02)
+    R, fin = run_reference(tmp_path, g, LAYER_ROWS, 4_000_000, 1796308352)
+    r = m.run([g], [m.OpticalProps.from_tissues(LAYER_ROWS)],
+              [m.Job(0, 0, 20_000_000, 4242, "uniform")], table=table)[0]
+    chi2, dof, pv = compare(r, R, fin, 16)
+    assert dof >= 200 and pv > 1e-4, (chi2, dof, pv)
+    total_ref = R.sum() / fin
+    total = r.drs.sum() / m.WEIGHT_SCALE / r.photons
+    sigma = np.sqrt(total * (1 - total) * (1 / fin + 1 / r.photons))
+    assert abs(total - total_ref) < 4 * sigma, (total, total_ref, sigma)
