@@ -75,3 +75,19 @@ def test_cli_absorption_and_transmission_maps(engine, tmp_path, table):
     rep = json.loads((tmp_path / "out_report.json").read_text())
     assert abs(A.sum() - rep["absorbed"] / 2 ** 32 / 5000) < 1e-9
     assert (tmp_path / "out_trans.bin").exists()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("math,steps", [("exact", "merged"), ("fast", "voxel"), ("f64", "merged")])
+def test_cli_math_and_step_modes(engine, tmp_path, table, math, steps):
+    """math= and steps= reach the engine: the CLI's tallies equal the library's"""
+    g, p = inputs(tmp_path)
+    engine.write_safeprimes(tmp_path / "safeprimes_base32.txt", table[:230401])
+    (tmp_path / "params.txt").write_text(f"photons=5000\nseed=77\nmath={math}\nsteps={steps}\n")
+    r = run([g, p, "params.txt", "out"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    drs, _, _ = read_drs_file(tmp_path / "out_drs.bin")
+    res = engine.run([engine.geometry_read_from_file(g)], [engine.opticalprops_read_from_file(p)],
+                     [engine.Job(0, 0, 5000, 77, "uniform")], table=table[:230401], math=math,
+                     steps=steps)[0]
+    assert np.array_equal(drs, res.drs.astype(np.float64) / engine.WEIGHT_SCALE / 5000)

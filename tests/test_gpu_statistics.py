@@ -166,3 +166,18 @@ def test_skin_model_runs(table):
     r = m.run([g], [p], [m.Job(0, 0, 200_000, 5, "uniform")], table=table)[0]
     assert r.photons == 200_000 and residual(r.totals) == 0
     assert 0 < r.totals["r_in"] < r.totals["w_launched"]
+
+
+@pytest.mark.parametrize("which", ["layered", "deep"])
+def test_full_size_invariants(table, which):
+    """the benchmark's full sizes, through size-independent properties: the
+    layered 256x256x128 job at 1e8 photons and the 1024x1024x256 grid (256 MB,
+    beyond L2) at 1e7 conserve weight exactly, their bins sum to the totals, and
+    every photon finishes (none at the step cap)"""
+    from ymc3d_b200.workloads import deep_grid, layered_vessel
+    w = layered_vessel(photons=100_000_000) if which == "layered" else deep_grid(photons=10_000_000)
+    r = m.run(w.geoms, w.props, w.jobs, table=table)[0]
+    t = r.totals
+    assert t["photons"] == w.jobs[0].photons and residual(t) == 0
+    assert int(r.drs.sum()) == t["r_in"] and int(r.trans.sum()) == t["t_in"]
+    assert t["capped"] == 0
