@@ -646,6 +646,11 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
     PhotonT<R> p;
     bool alive = false;
     int chunk = 0;
+    /* Loop iterations modulo the 45-step chunk.  A photon starts only at tick 0,
+     * as a reference slot starts only at a launch boundary: a lane whose photon
+     * ended waits out the rest of the chunk (the reference's masked steps), so
+     * the lanes of a warp reach their chunk ends on the same iteration. */
+    int tick = 0;
     uint32_t psteps = 0;
     uint32_t fresnel = 0;
     uint64_t qw0 = 0;
@@ -654,6 +659,10 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
 
     for (;;) {
         if (!alive) {
+            if (tick != 0) {
+                tick = (tick == MC3D_NUM_PHOTON_STEPS - 1) ? 0 : tick + 1;
+                continue;
+            }
             if (left == 0) {
                 if (P.cancel && *((volatile const int *)P.cancel)) break;
                 int64_t gs = (int64_t)atomicAdd((unsigned long long *)P.work_counter, 1ull);
@@ -707,6 +716,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
                                            &lat_mirror);
         chunk++;
         psteps++;
+        tick = (tick == MC3D_NUM_PHOTON_STEPS - 1) ? 0 : tick + 1;
 
         bool done = false;
         uint64_t lost = 0;
