@@ -45,11 +45,11 @@ OPS_JUMP = 8
 OPS_FRESNEL, SFU_FRESNEL = 37, 6
 FP32_LANES_PER_SM, SFU_LANES_PER_SM = 128, 16
 # DRAM bytes read + written by one photon-kernel launch of the layered workload
-# (ncu dram__bytes_read.sum + dram__bytes_write.sum = 30,480,128 + 1,825,792 on a
+# (ncu dram__bytes_read.sum + dram__bytes_write.sum = 30,560,768 + 2,696,448 on a
 # 1e7-photon launch, profiles/photon_kernel_fast_g1_layered_vessel_1e7_full.md):
 # the first touch of grid, packed cell map, table and tallies, independent of the
 # photon count
-TRAFFIC_BYTES_PER_LAUNCH = 32_305_920
+TRAFFIC_BYTES_PER_LAUNCH = 33_257_216
 
 
 def parse():
