@@ -15,11 +15,13 @@
  * including its quirks (Fresnel denominator, 0/0 -> transmit at normal incidence,
  * mirror short-circuit after a Fresnel reflection, freeze one step after entering
  * air, i/j/k re-derived from the position every 45 steps, the NaN/db==0 quickfix
- * at the end of each 45-step chunk).  The math policy decides how the elementary
- * operations are evaluated: MathExact uses correctly rounded IEEE operations and
- * the reproducible series of mc3d_exactmath.h (bit-identical to the CPU
- * transcription), MathFast uses the GPU's approximate instructions like the
- * reference's -use_fast_math build.
+ * at the end of each 45-step chunk).  The math policy fixes the transport type
+ * and how the elementary operations are evaluated: MathExact uses correctly
+ * rounded IEEE operations and the reproducible series of mc3d_exactmath.h
+ * (bit-identical to the CPU transcription), MathFast uses the GPU's approximate
+ * instructions like the reference's -use_fast_math build, MathF64 steps in FP64.
+ * With fast math the face crossings inside cubes of uniform tissue can be merged
+ * into one step (photon_step's JUMP).
  */
 #ifndef MC3D_ENGINE_CUH
 #define MC3D_ENGINE_CUH
@@ -183,8 +185,6 @@ struct MathF64 {
 #define MC3D_TISSUE_AIR 0
 #define MC3D_TAB_STRIDE 3 /* float4 per tissue in the optical table */
 
-/* fixed-point weight of the FP32 policies, 2^-32 resolution */
-static __device__ __forceinline__ uint64_t qw(float w) { return FloatTable::qw(w); }
 
 /* src/mc3d_gpu.cu:53-63 */
 template <class M, class R = typename M::real>
@@ -259,7 +259,6 @@ struct PhotonT {
     R x, y, z, ux, uy, uz, W, s;
     int i, j, k, tissue;
 };
-using Photon = PhotonT<float>;
 
 /* Per-thread tallies live in shared memory, one column per thread, so that the
  * step loop keeps only the photon in registers.  They are touched when a photon
