@@ -368,20 +368,25 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def run_reference_sweep(args, exe: Path):
-    """The reference binary once per wavelength of the sweep (uniform beam: its
-    pencil branch is compiled out), timed as the sum of its run_3dmc_gpu calls."""
-    from ymc3d_b200.workloads import sweep, write_geometry_file, write_optprops_file
-    w = sweep(photon_scale=args.photon_scale, beam="uniform")
-    g = w.geoms[0]
+def run_reference_batched(args, exe: Path):
+    """The reference binary once per job of a batched workload (uniform beam: its
+    pencil branch is compiled out), timed as the sum of its run_3dmc_gpu calls.
+    The reference runs at least 230,400 photons per call (one per slot)."""
+    from ymc3d_b200 import workloads as W
+    from ymc3d_b200.workloads import write_geometry_file, write_optprops_file
+    if args.workload == "sweep":
+        w = W.sweep(photon_scale=args.photon_scale, beam="uniform")
+    else:
+        w = W.uneven(photons=max(1, int(1e7 * args.photon_scale)))
     tmp = Path(tempfile.mkdtemp())
-    write_geometry_file(tmp / "geom.bin", g.tissue, g.dx, g.dy, g.dz)
+    for gi, g in enumerate(w.geoms):
+        write_geometry_file(tmp / f"geom{gi}.bin", g.tissue, g.dx, g.dy, g.dz)
     secs, fins = 0.0, 0
     for k, job in enumerate(w.jobs):
         p = w.props[job.props]
         rows = np.stack([p.mua, p.mus, p.g, p.n], 1)[1:]
         write_optprops_file(tmp / f"p{k}.bid", rows)
-        subprocess.run([str(exe), str(tmp / "geom.bin"), str(tmp / f"p{k}.bid"),
+        subprocess.run([str(exe), str(tmp / f"geom{job.geom}.bin"), str(tmp / f"p{k}.bid"),
                         str(int(job.photons)), str(int(job.seed) & 0xffffffff or 1),
                         str(tmp / f"r{k}"), str(exe.parent)], check=True,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
@@ -394,7 +399,7 @@ def run_reference_sweep(args, exe: Path):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": w.name, "jobs": len(w.jobs), "photons_per_step": fins,
                        "photon_scale": args.photon_scale,
-                       "how": "one run_3dmc_gpu call per wavelength, summed"},
+                       "how": "one run_3dmc_gpu call per job, summed"},
             "impl": "reference"}
     print(json.dumps(line), flush=True)
 
@@ -404,13 +409,21 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    if args.workload == "sweep":
+    if args.workload in ("homogeneous", "precision", "deep"):
+        why = {"homogeneous": "the workload's pencil beam is compiled out of the reference "
+                              "(src/mc3d_gpu.cu:87-95)",
+               "precision": "the reference has no FP64 stepping",
+               "deep": "a 1e7-photon deep-grid run takes the reference minutes; its "
+                       "per-photon cost is measured on the layered workload"}[args.workload]
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    if args.workload in ("sweep", "uneven"):
         exe = ROOT / "oracle" / "_ref" / "gpu-mc-ref"
         if not exe.exists():
             print(json.dumps({"impl": "reference", "unavailable":
                               "oracle/_ref/gpu-mc-ref not built (oracle/build_ref.py)"}))
             return
-        return run_reference_sweep(args, exe)
+        return run_reference_batched(args, exe)
     exe = ROOT / "oracle" / "_ref" / "gpu-mc-ref"
     if not exe.exists():
         print(json.dumps({"impl": "reference", "unavailable":
