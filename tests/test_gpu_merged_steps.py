@@ -92,7 +92,6 @@ def test_exact_math_ignores_step_mode(table):
     assert a.totals == b.totals and np.array_equal(a.drs, b.drs)
 
 
-
 def test_merged_steps_absorption_profile(table):
     """the absorption map books each interaction in the voxel where it happens:
     its depth profile agrees with per-face stepping"""
