@@ -53,14 +53,15 @@ enum mc3d_beam { MC3D_BEAM_UNIFORM = 0, MC3D_BEAM_PENCIL = 1 };
  * reference). */
 enum mc3d_math { MC3D_MATH_FAST = 0, MC3D_MATH_EXACT = 1, MC3D_MATH_F64 = 2 };
 
-/* Step decomposition of the fast-math kernel.  MERGED (the default) replaces the
- * voxel-face crossings of a flight through uniform tissue by one step to the
- * edge of a sphere known to hold only that tissue (a per-voxel safe-distance
- * map, built when the plan is created); each replaced crossing would only have
- * moved the photon.  VOXEL steps at every voxel face, as the reference does
- * (src/mc3d_gpu.cu:181-339).  Both are the reference's physics; the step counts
- * in mc3d_totals differ.  Exact math always steps at every face, and so does
- * a launch with a geometry of nx * ny * (nz + 63) >= 2^32 voxels. */
+/* Step decomposition of the fast-math kernel.  MERGED (the default) runs each
+ * step's voxel traversal on the cube of voxels around the photon's voxel that
+ * holds only its tissue (a per-voxel safe-distance map, built when the plan is
+ * created), so the face crossings inside that cube, each of which would only
+ * have moved the photon, become one step.  VOXEL steps at every voxel face, as
+ * the reference does (src/mc3d_gpu.cu:181-339).  Both are the reference's
+ * physics; the step counts in mc3d_totals differ.  Exact and FP64 math always
+ * step at every face, and so does a launch with a geometry of
+ * nx * ny * (nz + 63) >= 2^32 voxels. */
 enum mc3d_steps { MC3D_STEPS_MERGED = 0, MC3D_STEPS_VOXEL = 1 };
 
 /* Voxel geometry (geometry_t, src/mc3d_types.h:38-43), tissue indices as uint8
@@ -102,7 +103,8 @@ typedef struct {
  *   w_launched = r_in + r_out + t_in + t_out + absorbed + rr_killed - rr_created + lost */
 typedef struct {
     uint64_t photons;    /* photons finished */
-    uint64_t steps;      /* photon steps executed (iterations of src/mc3d_gpu.cu:175-340) */
+    uint64_t steps;      /* photon steps executed (iterations of src/mc3d_gpu.cu:175-340;
+                            a merged step counts once) */
     uint64_t w_launched; /* sum Q(1 - Rsp) */
     uint64_t r_in;       /* reflected, inside the surface grid (= sum of drs bins) */
     uint64_t r_out;      /* reflected, outside the grid */
