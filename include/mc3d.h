@@ -59,9 +59,9 @@ enum mc3d_math { MC3D_MATH_FAST = 0, MC3D_MATH_EXACT = 1, MC3D_MATH_F64 = 2 };
  * created), so the face crossings inside that cube, each of which would only
  * have moved the photon, become one step.  VOXEL steps at every voxel face, as
  * the reference does (src/mc3d_gpu.cu:181-339).  Both are the reference's
- * physics; the step counts in mc3d_totals differ.  Exact and FP64 math always
- * step at every face, and so does a launch with a geometry of
- * nx * ny * (nz + 63) >= 2^32 voxels. */
+ * physics; the step counts in mc3d_totals differ.  The mode applies to fast and
+ * FP64 math; exact math always steps at every face, and so does a launch with a
+ * geometry of nx * ny * (nz + 63) >= 2^32 voxels. */
 enum mc3d_steps { MC3D_STEPS_MERGED = 0, MC3D_STEPS_VOXEL = 1 };
 
 /* Voxel geometry (geometry_t, src/mc3d_types.h:38-43), tissue indices as uint8
@@ -150,7 +150,7 @@ typedef struct {
     int64_t max_steps;      /* per-photon step cap, 0 = 2^24 */
     mc3d_photon_record *photon_log; /* host, sum of photons over jobs, or NULL */
     volatile int32_t *cancel;       /* optional host flag, read when a stream starts */
-    int32_t steps;                  /* enum mc3d_steps (fast math only) */
+    int32_t steps;                  /* enum mc3d_steps (fast and FP64 math) */
     int32_t pad;
 } mc3d_options;
 

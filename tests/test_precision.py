@@ -48,12 +48,14 @@ def test_fast_fp32_engine_vs_fp64_oracle(table):
 
 
 @pytest.mark.gpu
-def test_f64_engine_vs_fp64_oracle(table):
+@pytest.mark.parametrize("steps", ["voxel", "merged"])
+def test_f64_engine_vs_fp64_oracle(table, steps):
     """the FP64 engine follows the FP64 transcription (statistically: CUDA's and
     libm's double functions differ in the last bit, and trajectories part)"""
     g, p = deep_like(48, 0.01, 0.01)
     o = run_oracle(g, p, 30000, 505, table, True)
-    r = m.run([g], [p], [m.Job(0, 0, 1_000_000, 606, "pencil")], table=table, math="f64")[0]
+    r = m.run([g], [p], [m.Job(0, 0, 1_000_000, 606, "pencil")], table=table, math="f64",
+              steps=steps)[0]
     assert residual(r.totals) == 0 and r.photons == 1_000_000
     chi2, dof, pv = drs_chi2(r.drs, r.drs_sq, r.photons, o["drs"], o["drs_sq"],
                              o["totals"]["photons"], f=4)
@@ -69,7 +71,8 @@ def test_fast_fp32_engine_vs_f64_engine(table, steps):
     stay within sampling error (chi-square) and the totals within 5 sigma"""
     g, p = deep_like(48, 0.01, 0.01)
     a = m.run([g], [p], [m.Job(0, 0, 2_000_000, 707, "pencil")], table=table, steps=steps)[0]
-    b = m.run([g], [p], [m.Job(0, 0, 2_000_000, 808, "pencil")], table=table, math="f64")[0]
+    b = m.run([g], [p], [m.Job(0, 0, 2_000_000, 808, "pencil")], table=table, math="f64",
+              steps=steps)[0]
     chi2, dof, pv = drs_chi2(a.drs, a.drs_sq, a.photons, b.drs, b.drs_sq, b.photons, f=2)
     assert dof > 100 and pv > 1e-4, (chi2, dof, pv)
     for key in ("r_in", "r_out", "t_in", "absorbed"):

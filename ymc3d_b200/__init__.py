@@ -323,9 +323,9 @@ def run(geoms: Sequence[Geometry], props: Sequence[OpticalProps], jobs: Sequence
     of one element, is read by the kernel whenever a thread takes a new stream: set
     it non-zero (from another thread) to stop; the call then raises
     MC3D_ERR_CANCELLED and the partial results are in the exception's .results.
-    `steps` (fast math): "merged" joins the face crossings of a flight through
-    uniform tissue into one step, "voxel" steps at every voxel face like the
-    reference; exact math always steps per face."""
+    `steps` (fast and FP64 math): "merged" joins the face crossings of a flight
+    through uniform tissue into one step, "voxel" steps at every voxel face like
+    the reference; exact math always steps per face."""
     table = default_table() if table is None else np.ascontiguousarray(table, dtype=np.uint32)
     g, p, j = _arrays(geoms, props, jobs)
     res, outs = _outs(geoms, jobs, absorption_map)

@@ -368,7 +368,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     /* ---- geometry grids and descriptors */
     std::vector<GeomDev> gh(ngeoms);
     p->d_grids.assign(ngeoms, nullptr);
-    p->jump = p->math == MC3D_MATH_FAST && opt.steps != MC3D_STEPS_VOXEL;
+    p->jump = p->math != MC3D_MATH_EXACT && opt.steps != MC3D_STEPS_VOXEL;
     /* the merged kernel indexes its cell map in 32 bits: larger grids step per face */
     for (int i = 0; i < ngeoms; i++)
         if ((uint64_t)geoms[i].nx * geoms[i].ny * ((uint64_t)geoms[i].nz + MC3D_SAFE_CAP) >=
@@ -515,7 +515,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     int bps = 0;
     PLAN_TRY(p->math == MC3D_MATH_FAST ? occupancy_photon_fast(p->block, p->smem, &bps, p->variant)
              : p->math == MC3D_MATH_EXACT ? occupancy_photon_exact(p->block, p->smem, &bps)
-                                          : occupancy_photon_f64(p->block, p->smem, &bps));
+                                          : occupancy_photon_f64(p->block, p->smem, &bps, p->variant));
     if (bps <= 0) {
         plan_free(p);
         return fail(MC3D_ERR_CAPACITY, "kernel does not fit an SM with block %d", opt.block);
@@ -564,7 +564,7 @@ static int plan_enqueue(mc3d_plan *p, cudaStream_t s)
         CUDA_TRY(launch_photon_fast(p->P, p->grid, p->block, p->smem, s, p->variant));
     else if (p->math == MC3D_MATH_EXACT)
         CUDA_TRY(launch_photon_exact(p->P, p->grid, p->block, p->smem, s));
-    else CUDA_TRY(launch_photon_f64(p->P, p->grid, p->block, p->smem, s));
+    else CUDA_TRY(launch_photon_f64(p->P, p->grid, p->block, p->smem, s, p->variant));
     return MC3D_OK;
 }
 

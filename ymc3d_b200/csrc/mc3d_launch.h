@@ -23,9 +23,9 @@ cudaError_t launch_photon_fast(const KernelParams &P, int grid, int block, size_
 cudaError_t launch_photon_exact(const KernelParams &P, int grid, int block, size_t smem,
                                 cudaStream_t stream);
 cudaError_t launch_photon_f64(const KernelParams &P, int grid, int block, size_t smem,
-                              cudaStream_t stream);
+                              cudaStream_t stream, int variant);
 cudaError_t occupancy_photon_fast(int block, size_t smem, int *blocks_per_sm, int variant);
-cudaError_t occupancy_photon_f64(int block, size_t smem, int *blocks_per_sm);
+cudaError_t occupancy_photon_f64(int block, size_t smem, int *blocks_per_sm, int variant);
 cudaError_t smem_limit_photon_f64(size_t smem);
 cudaError_t attributes_photon_f64(cudaFuncAttributes *attr);
 cudaError_t occupancy_photon_exact(int block, size_t smem, int *blocks_per_sm);
