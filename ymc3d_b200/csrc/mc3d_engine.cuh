@@ -652,9 +652,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
     int tick = 0;
     uint32_t psteps = 0;
     uint32_t fresnel = 0;
-    uint64_t qw0 = 0;
     unsigned long long *amap = nullptr;
-    const int64_t max_steps = P.max_steps;
 
     for (;;) {
         if (!alive) {
@@ -697,7 +695,6 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
             R rsp = M::div(n0 - n1, n0 + n1);
             rsp = rsp * rsp;
             p.W = (R)1 - rsp;
-            qw0 = M::qw(p.W);
             p.s = -M::log((R)mc3d_rand_oc(&rx, ra));
             derive_cell<M, JUMP>(g, p);
             chunk = 0;
@@ -741,7 +738,7 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
                 chunk = 0;
             }
         }
-        if (!done && (int64_t)psteps >= max_steps) {
+        if (!done && (int64_t)psteps >= P.max_steps) {
             lost = M::qw(p.W);
             p.W = 0;
             acc[T_CAPPED]++;
@@ -767,6 +764,11 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
                 if (inside && q) atomicAdd(P.trans + bin, (unsigned long long)q);
             }
             acc[slot] += q;
+            /* the launch weight 1 - Rsp again, as at the photon's start */
+            const R n0 = M::n(tab + MC3D_TAB_STRIDE * MC3D_TISSUE_AIR), n1 = M::n(tab + MC3D_TAB_STRIDE);
+            R rsp = M::div(n0 - n1, n0 + n1);
+            rsp = rsp * rsp;
+            const uint64_t qw0 = M::qw((R)1 - rsp);
             acc[T_W_LAUNCHED] += qw0;
             acc[T_ABSORBED] += qw0 - q - lost;
             acc[T_LOST] += lost;
