@@ -7,7 +7,6 @@ import re
 import subprocess
 
 import numpy as np
-import pytest
 
 from conftest import ROOT, has_gpu
 

@@ -7,7 +7,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT, has_gpu
+from conftest import ROOT
 from ymc3d_b200.workloads import read_drs_file, write_geometry_file, write_optprops_file
 
 CLI = ROOT / "ymc3d_b200" / "gpu-mc"

@@ -13,7 +13,6 @@ import hashlib
 import json
 import os
 import time
-from pathlib import Path
 
 from . import HERE, Job, Plan, default_table
 
