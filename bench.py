@@ -37,7 +37,7 @@ sys.path.insert(0, str(ROOT))
 # sin/cos counted once, integer and select operations not counted).  Of the 152,
 # 20 are special-function class (13 divisions, 2 sqrt, 2 rsqrt, 1 log, sin+cos of
 # sincospif); a Fresnel event (:226-257) adds 37, 6 of them special (acos, sin,
-# sqrt, 3 divisions).  The per-term breakdown is in DESIGN.md.
+# sqrt, 3 divisions).
 OPS_STEP, SFU_STEP = 152, 20
 # a merged step adds the jump: radius x unit, compare, 3 x (x + u R)
 OPS_JUMP = 8
@@ -45,9 +45,8 @@ OPS_FRESNEL, SFU_FRESNEL = 37, 6
 FP32_LANES_PER_SM, SFU_LANES_PER_SM = 128, 16
 # DRAM bytes read + written by one photon-kernel launch of the layered workload
 # (ncu dram__bytes_read.sum + dram__bytes_write.sum = 30,560,768 + 2,696,448 on a
-# 1e7-photon launch, profiles/photon_kernel_fast_g1_layered_vessel_1e7_full.md):
-# the first touch of grid, packed cell map, table and tallies, independent of the
-# photon count
+# 1e7-photon launch): the first touch of grid, packed cell map, table and tallies,
+# independent of the photon count
 TRAFFIC_BYTES_PER_LAUNCH = 33_257_216
 
 
@@ -182,6 +181,7 @@ def run_ours(args):
     import torch
 
     import ymc3d_b200 as m
+    from ymc3d_b200.shard import all_reduce_results
     from ymc3d_b200.workloads import layered_vessel
 
     world, rank, local, dist = dist_setup(args)
@@ -230,18 +230,7 @@ def run_ours(args):
         """sum the shards' integer tallies over NCCL (the path's exchange step)"""
         if world == 1:
             return res
-        r = res[0]
-        t = torch.from_numpy(np.concatenate([r.drs.view(np.int64).reshape(-1),
-                                             r.drs_sq.view(np.int64).reshape(-1),
-                                             r.trans.view(np.int64).reshape(-1),
-                                             np.array([r.totals[k] for k in m.TOTAL_FIELDS],
-                                                      np.uint64).view(np.int64)])).cuda(dev)
-        dist.all_reduce(t)
-        a = t.cpu().numpy().view(np.uint64)
-        r.drs, r.drs_sq, r.trans = (a[:nb].reshape(r.drs.shape), a[nb:2 * nb].reshape(r.drs.shape),
-                                    a[2 * nb:3 * nb].reshape(r.drs.shape))
-        r.totals = {k: int(v) for k, v in zip(m.TOTAL_FIELDS, a[3 * nb:])}
-        return res
+        return all_reduce_results(res, device=torch.device("cuda", dev))
 
     for k in range(args.warmup):
         warm_plan.execute(stream.cuda_stream)

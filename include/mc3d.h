@@ -216,9 +216,11 @@ int mc3d_safe_distance(const uint8_t *tissue, int32_t nx, int32_t ny, int32_t nz
  * static device array of MC3D_NOALLOC_SCRATCH_BYTES that every GPU loading the
  * library holds until exit; inputs beyond its limits return MC3D_ERR_CAPACITY.
  * All calls share that array: calls whose work overlaps on the GPU race, so run
- * them one after another (the call returns once the kernel is queued on `stream`).
- * The first call on a device looks up the array's address and should come before
- * any stream capture. */
+ * them one after another.  Before its launch the call synchronises `stream` (it
+ * reads back the grid's largest tissue index and the seeding scan), so the host
+ * waits for the work already queued there; it returns once the photon kernel is
+ * queued.  The first call on a device looks up the array's address and should
+ * come before any stream capture.  The caller's current device is restored. */
 #define MC3D_NOALLOC_SCRATCH_BYTES (1u << 20)
 #define MC3D_NOALLOC_MAX_TABLE 230401     /* safe-prime table lines */
 #define MC3D_NOALLOC_MAX_TISSUES 256

@@ -94,3 +94,30 @@ def test_reference_shaped_entry_needs_table(engine, tmp_path, monkeypatch):
     st = engine.lib().mc3d_run_3dmc_gpu(geo, props, 100, R.ctypes.data, None, None, None, None,
                                         C.byref(fin))
     assert st == -6
+
+
+def test_noalloc_rejects_non_finite_values(engine, table):
+    """mc3d_run_noalloc checks voxel sizes and optical values like mc3d_run, before
+    it touches the device (the pointers below are never dereferenced)"""
+    g, p = _inputs(engine)
+    lib = engine.lib()
+    fake = C.c_void_p(0x1000)  # non-null stand-in for device buffers
+    tab = np.ascontiguousarray(table[:1000])
+    cj = engine.Job(0, 0, 10, 1796308352, "uniform").c()
+
+    def call(cg, cp):
+        return lib.mc3d_run_noalloc(C.byref(cg), C.byref(cp), C.byref(cj), tab.ctypes.data,
+                                    len(tab), 0, None, fake, fake, fake, fake)
+
+    cp = p.c()
+    for bad in (float("inf"), float("nan")):
+        for axis in range(3):
+            d = [0.1, 0.1, 0.1]
+            d[axis] = bad
+            assert call(engine.CGeom(4, 4, 4, 0, *d, 0x1000), cp) == -2
+    cg = engine.CGeom(4, 4, 4, 0, 0.1, 0.1, 0.1, 0x1000)
+    for field in ("mua", "mus", "g", "n"):
+        for bad in (float("inf"), float("nan")):
+            q = engine.OpticalProps(p.mua.copy(), p.mus.copy(), p.g.copy(), p.n.copy())
+            getattr(q, field)[1] = bad
+            assert call(cg, q.c()) == -4

@@ -105,3 +105,34 @@ def test_merged_steps_absorption_profile(table):
     big = b > 0.01 * b.max()
     assert big.sum() > 5
     assert np.max(np.abs(a[big] - b[big]) / b[big]) < 0.05
+
+
+def deep_like(nx=512, ny=512, nz=64, d=0.01):
+    """a long-path, high-albedo medium like the deep-grid workload, one tissue"""
+    g = m.Geometry(np.ones((nz, ny, nx), np.uint8), d, d, d)
+    return g, m.OpticalProps.from_tissues([(0.001, 20.0, 0.9, 1.4)])
+
+
+def test_merged_quickfix_loss_matches_voxel_steps(table):
+    """The reference's end-of-chunk quickfix (src/mc3d_gpu.cu:343-353) kills a photon
+    whose 45th step had db == 0: in float a scattering move can round onto a voxel
+    face, and when the new direction points back across it the next one-voxel DDA
+    gives 0.  On long-path media that costs a few 1e-3 of the launched weight.
+    Merged steps evaluate the same one-voxel condition at the chunk's last step, so
+    they lose as many photons and as much weight as per-face steps (within Poisson
+    error), although the merged box itself rarely has a zero boundary distance."""
+    g, p = deep_like()
+    n = 1_000_000
+    mer = m.run([g], [p], [m.Job(0, 0, n, 61, "uniform")], table=table)[0]
+    vox = m.run([g], [p], [m.Job(0, 0, n, 62, "uniform")], table=table, steps="voxel")[0]
+    qm, qv = mer.totals["quickfix"], vox.totals["quickfix"]
+    assert qv > 1000, qv
+    assert abs(qm - qv) < 4 * np.sqrt(qm + qv), (qm, qv)
+    lm = mer.totals["lost"] / m.WEIGHT_SCALE / n
+    lv = vox.totals["lost"] / m.WEIGHT_SCALE / n
+    assert lv > 1e-4
+    # each lost weight is at most 1: the Poisson count bounds the variance
+    assert abs(lm - lv) < 4 * np.sqrt(qm + qv) / n, (lm, lv)
+    for key in ("r_in", "r_out", "absorbed"):
+        assert abs(total_z(mer.totals, vox.totals, key)) < 5, key
+    assert residual(mer.totals) == 0 and residual(vox.totals) == 0

@@ -528,12 +528,24 @@ static __device__ __forceinline__ bool finite_state(const PhotonT<R> &p)
            isfinite(p.ux) && isfinite(p.uy) && isfinite(p.uz);
 }
 
-/* The NaN/Inf/db==0 quickfix run after each 45-step launch (src/mc3d_gpu.cu:343-353).
- * Returns true (and zeroes the photon) when it fires. */
-template <class R>
-static __device__ __forceinline__ bool quickfix(PhotonT<R> &p, R db)
+/* The boundary distance the reference's one-voxel DDA (src/mc3d_gpu.cu:29-49,
+ * :194) gives a step that starts in state p.  It is 0 when the photon sits on a
+ * face of its voxel and moves out through it, which happens when a scattering
+ * move rounds onto a voxel face and the new direction points back across it. */
+template <class M, class R = typename M::real>
+static __device__ __forceinline__ R voxel_db(const GeomDev &g, const PhotonT<R> &p)
 {
-    if (!finite_state(p) || db == 0) {
+    R x = p.x, y = p.y, z = p.z;
+    return intersection<M>(g, p.i, p.j, p.k, &x, p.ux, &y, p.uy, &z, p.uz);
+}
+
+/* The NaN/Inf/db==0 quickfix run after each 45-step launch (src/mc3d_gpu.cu:343-353);
+ * zero_db tells whether the launch's last step had db == 0.  Returns true (and
+ * zeroes the photon) when it fires. */
+template <class R>
+static __device__ __forceinline__ bool quickfix(PhotonT<R> &p, bool zero_db)
+{
+    if (!finite_state(p) || zero_db) {
         p.x = 0; p.y = 0; p.z = 0;
         p.ux = 0; p.uy = 0; p.uz = 1;
         p.W = 0; p.s = 0;
@@ -708,6 +720,13 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
         R db;
         bool lat_mirror;
         bool froze;
+        /* Merged steps: the quickfix must see the boundary distance of the
+         * reference's one-voxel DDA for the chunk's last step, not the merged
+         * box's (which is never 0 inside a uniform cube), or merged steps would
+         * lose less weight to it than the reference does.  Taken from that
+         * step's start state. */
+        bool vzero = false;
+        if (JUMP && chunk == MC3D_NUM_PHOTON_STEPS - 1) vzero = voxel_db<M>(g, p) == 0;
         froze = photon_step<M, AMAP, JUMP>(g, tab, p, rx, ra, acc, &db, &fresnel, amap,
                                            &lat_mirror);
         chunk++;
@@ -719,15 +738,25 @@ __device__ __forceinline__ void photon_kernel_body(const KernelParams &P)
         if (froze) {
             /* If the freeze step's mirror did not fire and the photon is off the
              * lateral faces, the masked steps change nothing and see the freeze
-             * step's boundary distance again: no need to replay them. */
-            if (lat_mirror || !(p.x > 0 && p.x < g.Lx && p.y > 0 && p.y < g.Ly))
-                db = masked_steps<M>(g, p, MC3D_NUM_PHOTON_STEPS - chunk, db);
+             * step's boundary distance again: no need to replay them.  The
+             * replayed masked steps are one-voxel steps; without them a merged
+             * kernel takes the one-voxel distance of the frozen state, which is
+             * the freeze step's start state. */
+            bool zero;
+            if (lat_mirror || !(p.x > 0 && p.x < g.Lx && p.y > 0 && p.y < g.Ly)) {
+                if (chunk < MC3D_NUM_PHOTON_STEPS)
+                    zero = masked_steps<M>(g, p, MC3D_NUM_PHOTON_STEPS - chunk, db) == 0;
+                else
+                    zero = JUMP ? vzero : db == 0;
+            } else {
+                zero = JUMP ? voxel_db<M>(g, p) == 0 : db == 0;
+            }
             R w_before = p.W;
-            if (quickfix(p, db)) { acc[T_QUICKFIX]++; lost = M::qw(w_before); }
+            if (quickfix(p, zero)) { acc[T_QUICKFIX]++; lost = M::qw(w_before); }
             done = true;
         } else if (chunk == MC3D_NUM_PHOTON_STEPS) {
             R w_before = p.W;
-            if (quickfix(p, db)) {
+            if (quickfix(p, JUMP ? vzero : db == 0)) {
                 acc[T_QUICKFIX]++;
                 lost = M::qw(w_before);
                 done = true;

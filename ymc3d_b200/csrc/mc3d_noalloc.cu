@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -135,8 +136,15 @@ extern "C" int mc3d_run_noalloc(const mc3d_geom *geom, const mc3d_props *props,
     if (props->num_tissue_types < 2 || props->num_tissue_types > MC3D_NOALLOC_MAX_TISSUES)
         return nfail(MC3D_ERR_CAPACITY, "num_tissue_types outside 2..MC3D_NOALLOC_MAX_TISSUES");
     if (geom->nx <= 0 || geom->ny <= 0 || geom->nz <= 0 || !(geom->dx > 0) || !(geom->dy > 0) ||
-        !(geom->dz > 0))
-        return nfail(MC3D_ERR_GEOMETRY, "bad geometry size");
+        !(geom->dz > 0) || !std::isfinite(geom->dx) || !std::isfinite(geom->dy) ||
+        !std::isfinite(geom->dz))
+        return nfail(MC3D_ERR_GEOMETRY, "bad geometry size or voxel size");
+    /* the same value checks as mc3d_plan_create: a non-finite coefficient would
+     * step NaN positions and fill the tallies with garbage */
+    for (int t = 0; t < props->num_tissue_types; t++)
+        if (!std::isfinite(props->mua[t]) || !std::isfinite(props->mus[t]) ||
+            !std::isfinite(props->g[t]) || !std::isfinite(props->n[t]))
+            return nfail(MC3D_ERR_PROPS, "a tissue's optical property is not finite");
     for (int64_t i = 0; i < table_len; i++)
         if (table[i] < 2u) return nfail(MC3D_ERR_TABLE, "table holds a multiplier below 2");
     if (job->photons < 0 || job->streams < 0 || (job->beam != 0 && job->beam != 1))
@@ -151,6 +159,13 @@ extern "C" int mc3d_run_noalloc(const mc3d_geom *geom, const mc3d_props *props,
     if (first < 0 || count < 0 || first + count > S)
         return nfail(MC3D_ERR_ARG, "stream range outside the job");
 
+    /* the caller's current device is put back on every return */
+    int prev_device = 0;
+    NA_TRY(cudaGetDevice(&prev_device));
+    struct DeviceGuard {
+        int prev;
+        ~DeviceGuard() { cudaSetDevice(prev); }
+    } guard{prev_device};
     NA_TRY(cudaSetDevice(device));
     unsigned char *base = nullptr;
     int st = scratch_address(device, &base);
