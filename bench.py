@@ -74,6 +74,12 @@ def parse():
                     help="beam of the sweep workload (the reference has only uniform)")
     ap.add_argument("--photon-scale", type=float, default=0.01,
                     help="photon budget factor of the sweep / uneven / deep workloads")
+    ap.add_argument("--sweep-scale", type=float, default=1.0,
+                    help="photon budget factor of the sweep object of the default run")
+    ap.add_argument("--no-sweep", action="store_true",
+                    help="leave the sweep object out of the default run")
+    ap.add_argument("--sweep-ref-batches", type=int, default=4,
+                    help="reference arm: seeded runs per sweep job, for batch-means sigma")
     return ap.parse_args()
 
 
@@ -350,10 +356,183 @@ def run_ours(args):
         line["cpu_baseline"] = cpu_baseline(w, args.cpu_seconds)
     plan.close()
     warm_plan.close()
+    if world == 1 and not args.no_sweep:
+        sw = measure_sweep(args, dev, stream, flush)
+        sfu = (sw["_steps"] * SFU_STEP + sw["_fresnel"] * SFU_FRESNEL) / sw["_seconds"]
+        sw["roofline"] = {"bound": "sfu", "achieved": sfu / 1e9, "peak": sfu_peak / 1e9,
+                          "unit": "Gop/s", "frac": sfu / sfu_peak}
+        for k in ("_steps", "_fresnel", "_seconds"):
+            sw.pop(k)
+        sw["gpu_launches"] = 1 + sw["jobs"]  # the batched launch, then one per job
+        line["sweep"] = sw
     print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+SWEEP_STRATA = 8
+
+
+def sweep_subset(w, strata: int = SWEEP_STRATA, seed: int = 20240611) -> list[int]:
+    """A seeded stratified subset of the sweep's jobs for the reference arm: the jobs
+    sorted by mua (which sets a photon's path length) in `strata` equal strata, one
+    job drawn from each."""
+    mua = np.array([float(w.props[j.props].mua[1]) for j in w.jobs])
+    order = np.argsort(mua, kind="stable")
+    rng = np.random.Generator(np.random.PCG64(seed))
+    per = len(order) // strata
+    return [int(order[s * per + int(rng.integers(per))]) for s in range(strata)]
+
+
+def sweep_strata(w, strata: int = SWEEP_STRATA) -> list[list[int]]:
+    mua = np.array([float(w.props[j.props].mua[1]) for j in w.jobs])
+    order = np.argsort(mua, kind="stable")
+    per = len(order) // strata
+    return [[int(k) for k in order[s * per:(s + 1) * per]] for s in range(strata)]
+
+
+def r_total_sigma(r) -> tuple[float, float]:
+    """total diffuse reflectance per photon and its standard error; each photon's
+    reflected weight lands in one bin, so the bins' sum W^2 is the photons' sum W^2"""
+    n = max(1, r.photons)
+    m1 = float(r.drs.sum()) / 4294967296.0 / n
+    m2 = float(r.drs_sq.sum()) / 4294967296.0 / n
+    return m1, float(np.sqrt(max(m2 - m1 * m1, 0.0) / n))
+
+
+def measure_sweep(args, dev, stream, flush) -> dict:
+    """The metric's own comparison on the hyperspectral sweep: 128 optical tables on
+    the homogeneous 64^3 x 0.1 mm geometry, photons log-uniform in [1e6, 1e8] per
+    job (2.75e9 in all at scale 1), uniform beam (the reference's only beam).
+    Batched = one persistent launch over every job; plain = one launch per job with
+    the same jobs and seeds.  Both give identical tallies (checked word for word),
+    so their DRS sigma-errors are equal by construction."""
+    import torch
+
+    import ymc3d_b200 as m
+    from ymc3d_b200 import workloads as W
+
+    w = W.sweep(photon_scale=args.sweep_scale, beam="uniform")
+    warm = W.sweep(photon_scale=1e-3, beam="uniform")
+    wp = m.Plan(warm.geoms, warm.props, warm.jobs, device=dev, steps=args.step_mode)
+    wp.execute(stream.cuda_stream)
+    wp.read()
+    wp.close()
+
+    def timed(plan):
+        flush.fill_(7)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.execute(stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    with ClockSampler(dev) as clocks:
+        plan = m.Plan(w.geoms, w.props, w.jobs, device=dev, steps=args.step_mode)
+        t_batch = timed(plan)
+        batched = plan.read()
+        plan.close()
+        t_plain, identical = [], True
+        for k, job in enumerate(w.jobs):
+            pl = m.Plan([w.geoms[0]], [w.props[job.props]],
+                        [m.Job(0, 0, job.photons, job.seed, job.beam)], device=dev,
+                        steps=args.step_mode)
+            t_plain.append(timed(pl))
+            r = pl.read()[0]
+            pl.close()
+            b = batched[k]
+            identical &= (r.totals == b.totals and np.array_equal(r.drs, b.drs)
+                          and np.array_equal(r.drs_sq, b.drs_sq))
+    photons = sum(r.photons for r in batched)
+    steps = sum(r.totals["steps"] for r in batched)
+    fresnel = sum(r.totals["fresnel"] for r in batched)
+    rel = [sg / mu for mu, sg in map(r_total_sigma, batched) if mu > 0]
+    sub = sweep_subset(w)
+    return {"workload": w.name, "jobs": len(w.jobs), "photons": photons,
+            "photon_scale": args.sweep_scale, "beam": "uniform", "step_mode": args.step_mode,
+            "batched": {"value": photons / t_batch, "unit": "photons/s", "seconds": t_batch,
+                        "how": "one persistent launch over all jobs (tally clear + kernel), "
+                               "CUDA events, L2 flushed before"},
+            "plain": {"value": photons / sum(t_plain), "unit": "photons/s",
+                      "seconds": sum(t_plain),
+                      "how": "one launch per job, same jobs and seeds, CUDA events summed, "
+                             "L2 flushed before each"},
+            "batched_over_plain": sum(t_plain) / t_batch,
+            "tallies_identical": bool(identical),
+            "sigma": {"r_total_rel_median": float(np.median(rel)),
+                      "r_total_rel_max": float(np.max(rel)),
+                      "how": "per job from sum W^2; batched and plain are identical, so "
+                             "their sigma is equal"},
+            "steps_per_s": steps / t_batch, "fresnel_per_s": fresnel / t_batch,
+            "reference_subset": {
+                "jobs": sub, "photons": int(sum(w.jobs[k].photons for k in sub)),
+                "plain_seconds": float(sum(t_plain[k] for k in sub)),
+                "r_total": [list(r_total_sigma(batched[k])) for k in sub],
+                "how": "the jobs the reference arm runs (seeded, one per mua stratum); "
+                       "this engine's plain time on them"},
+            "clocks": clocks.summary(), "_steps": steps, "_fresnel": fresnel,
+            "_seconds": t_batch}
+
+
+def reference_sweep(args, exe: Path) -> dict:
+    """The reference's run_3dmc_gpu on the stratified subset of the sweep at the
+    jobs' full photon counts, each job as `--sweep-ref-batches` seeded runs whose
+    total-reflectance batch means give its sigma.  The reference's time for the whole
+    sweep is estimated by strata: each stratum's photons times its drawn job's
+    seconds per photon."""
+    from ymc3d_b200 import workloads as W
+    from ymc3d_b200.workloads import write_geometry_file, write_optprops_file
+    w = W.sweep(photon_scale=args.sweep_scale, beam="uniform")
+    sub = sweep_subset(w)
+    strata = sweep_strata(w)
+    tmp = Path(tempfile.mkdtemp())
+    g = w.geoms[0]
+    write_geometry_file(tmp / "geom.bin", g.tissue, g.dx, g.dy, g.dz)
+    nb = max(1, args.sweep_ref_batches)
+    jobs, t_est, fin_all, sec_all = [], 0.0, 0, 0.0
+    for s_idx, k in enumerate(sub):
+        job = w.jobs[k]
+        p = w.props[job.props]
+        write_optprops_file(tmp / f"p{k}.bid", np.stack([p.mua, p.mus, p.g, p.n], 1)[1:])
+        per = -(-int(job.photons) // nb)
+        rb, fins, secs = [], 0, 0.0
+        for b in range(nb):
+            seed = (int(job.seed) + 1000003 * b) & 0xFFFFFFFF or 1
+            out = tmp / f"s{k}_{b}"
+            subprocess.run([str(exe), str(tmp / "geom.bin"), str(tmp / f"p{k}.bid"), str(per),
+                            str(seed), str(out), str(exe.parent)], check=True,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            raw = Path(str(out) + "_ref.bin").read_bytes()
+            fin = int(np.frombuffer(raw, "<i8", 1)[0])
+            sec = float(np.frombuffer(raw, "<f8", 1, offset=8)[0])
+            nx, ny = np.frombuffer(raw, "<i4", 2, offset=16)
+            R = np.frombuffer(raw, "<f8", int(nx * ny), offset=24)
+            rb.append(float(R.sum()) / fin)
+            fins += fin
+            secs += sec
+        mean = float(np.mean(rb))
+        sig = float(np.std(rb, ddof=1) / np.sqrt(nb)) if nb > 1 else None
+        jobs.append({"job": k, "mua": float(p.mua[1]), "photons_requested": int(job.photons),
+                     "photons_finished": fins, "seconds": secs, "r_total": mean,
+                     "r_total_sigma_batch_means": sig})
+        fin_all += fins
+        sec_all += secs
+        stratum_photons = sum(int(w.jobs[j].photons) for j in strata[s_idx])
+        t_est += stratum_photons * secs / fins
+    return {"workload": w.name, "jobs_total": len(w.jobs), "photons_total": w.photons,
+            "photon_scale": args.sweep_scale, "beam": "uniform",
+            "subset": {"jobs": jobs, "photons": fin_all, "seconds": sec_all,
+                       "value": fin_all / sec_all, "unit": "photons/s",
+                       "how": f"one seeded job per mua stratum ({SWEEP_STRATA} strata of "
+                              f"{len(w.jobs) // SWEEP_STRATA}), full photon count, "
+                              f"{nb} run_3dmc_gpu calls per job, wall time of each call"},
+            "full_sweep_estimate": {"seconds": t_est, "value": w.photons / t_est,
+                                    "unit": "photons/s",
+                                    "how": "each stratum's photons x its drawn job's seconds "
+                                           "per finished photon"}}
 
 
 def run_reference_batched(args, exe: Path):
@@ -446,17 +625,23 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded layered-tissue geometry, reference input formats)",
         "config": {"workload": w.name, "photons_per_step": int(args.ref_photons),
+                   "photons_per_step_note": "1e7 per step against the engine arm's 1e8, so "
+                                            "that 20 steps end within minutes; the "
+                                            "reference's fixed 230,400-slot drain tail "
+                                            "weighs a little more at 1e7",
                    "voxels": list(g.shape), "voxel_mm": g.dx, "beam": "uniform",
                    "parallelism": "single GPU (the reference has no multi-GPU path)"},
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "photons/s", "cores": cores,
-                         "kind": "reference",
-                         "sample": f"{int(args.ref_photons)} photons per step through the "
-                                   "reference's run_3dmc_gpu (its CUDA kernels on cuda:0, its "
-                                   "OpenMP host tally), wall time of the call"},
+        "reference_run": {"value": value, "unit": "photons/s", "kind": "reference GPU binary",
+                          "device": "cuda:0", "host_cores": cores,
+                          "sample": f"{int(args.ref_photons)} photons per step through the "
+                                    "reference's run_3dmc_gpu (its CUDA kernels on cuda:0, its "
+                                    "OpenMP host tally), wall time of the call"},
         "e2e": {"value": value, "unit": "photons/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if world == 1 and not args.no_sweep:
+        line["sweep"] = reference_sweep(args, exe)
     print(json.dumps(line), flush=True)
 
 
