@@ -78,8 +78,11 @@ def parse():
                     help="photon budget factor of the sweep object of the default run")
     ap.add_argument("--no-sweep", action="store_true",
                     help="leave the sweep object out of the default run")
-    ap.add_argument("--sweep-ref-batches", type=int, default=4,
-                    help="reference arm: seeded runs per sweep job, for batch-means sigma")
+    ap.add_argument("--sweep-ref-seconds", type=float, default=30.0,
+                    help="reference arm: time budget per sampled sweep job (its four seeded "
+                         "calls, whose batch means give sigma)")
+    ap.add_argument("--ref-warmup-photons", type=float, default=230400,
+                    help="reference arm: photons of each warm-up call (the slot count)")
     return ap.parse_args()
 
 
@@ -478,11 +481,12 @@ def measure_sweep(args, dev, stream, flush) -> dict:
 
 
 def reference_sweep(args, exe: Path) -> dict:
-    """The reference's run_3dmc_gpu on the stratified subset of the sweep at the
-    jobs' full photon counts, each job as `--sweep-ref-batches` seeded runs whose
-    total-reflectance batch means give its sigma.  The reference's time for the whole
-    sweep is estimated by strata: each stratum's photons times its drawn job's
-    seconds per photon."""
+    """The reference's run_3dmc_gpu on the stratified subset of the sweep.  Each
+    sampled job runs as four seeded calls (batch means give its sigma): a pilot of
+    230,400 photons (the reference's slot count and minimum), then three calls
+    sized from the pilot's rate to fill --sweep-ref-seconds, never beyond the job's
+    own photon count.  The reference's time for the whole sweep is estimated by
+    strata: each stratum's photons times its sampled job's seconds per photon."""
     from ymc3d_b200 import workloads as W
     from ymc3d_b200.workloads import write_geometry_file, write_optprops_file
     w = W.sweep(photon_scale=args.sweep_scale, beam="uniform")
@@ -491,33 +495,44 @@ def reference_sweep(args, exe: Path) -> dict:
     tmp = Path(tempfile.mkdtemp())
     g = w.geoms[0]
     write_geometry_file(tmp / "geom.bin", g.tissue, g.dx, g.dy, g.dz)
-    nb = max(1, args.sweep_ref_batches)
+    slots = 230_400
+
+    def call(k, photons, seed, tag):
+        out = tmp / f"s{k}_{tag}"
+        subprocess.run([str(exe), str(tmp / "geom.bin"), str(tmp / f"p{k}.bid"), str(photons),
+                        str(seed), str(out), str(exe.parent)], check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        raw = Path(str(out) + "_ref.bin").read_bytes()
+        fin = int(np.frombuffer(raw, "<i8", 1)[0])
+        sec = float(np.frombuffer(raw, "<f8", 1, offset=8)[0])
+        nx, ny = np.frombuffer(raw, "<i4", 2, offset=16)
+        R = np.frombuffer(raw, "<f8", int(nx * ny), offset=24)
+        return fin, sec, float(R.sum()) / fin
+
     jobs, t_est, fin_all, sec_all = [], 0.0, 0, 0.0
     for s_idx, k in enumerate(sub):
         job = w.jobs[k]
         p = w.props[job.props]
         write_optprops_file(tmp / f"p{k}.bid", np.stack([p.mua, p.mus, p.g, p.n], 1)[1:])
-        per = -(-int(job.photons) // nb)
-        rb, fins, secs = [], 0, 0.0
-        for b in range(nb):
-            seed = (int(job.seed) + 1000003 * b) & 0xFFFFFFFF or 1
-            out = tmp / f"s{k}_{b}"
-            subprocess.run([str(exe), str(tmp / "geom.bin"), str(tmp / f"p{k}.bid"), str(per),
-                            str(seed), str(out), str(exe.parent)], check=True,
-                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
-            raw = Path(str(out) + "_ref.bin").read_bytes()
-            fin = int(np.frombuffer(raw, "<i8", 1)[0])
-            sec = float(np.frombuffer(raw, "<f8", 1, offset=8)[0])
-            nx, ny = np.frombuffer(raw, "<i4", 2, offset=16)
-            R = np.frombuffer(raw, "<f8", int(nx * ny), offset=24)
-            rb.append(float(R.sum()) / fin)
-            fins += fin
-            secs += sec
-        mean = float(np.mean(rb))
-        sig = float(np.std(rb, ddof=1) / np.sqrt(nb)) if nb > 1 else None
-        jobs.append({"job": k, "mua": float(p.mua[1]), "photons_requested": int(job.photons),
-                     "photons_finished": fins, "seconds": secs, "r_total": mean,
-                     "r_total_sigma_batch_means": sig})
+        seeds = [((int(job.seed) + 1000003 * b) & 0xFFFFFFFF) or 1 for b in range(4)]
+        runs = [call(k, slots, seeds[0], 0)]
+        rate = runs[0][0] / runs[0][1]
+        left = max(0, int(job.photons) - runs[0][0])
+        per = max(slots, min(left, int(rate * max(0.0, args.sweep_ref_seconds - runs[0][1])))
+                  // 3)
+        for b in (1, 2, 3):
+            runs.append(call(k, per, seeds[b], b))
+        fins = sum(r[0] for r in runs)
+        secs = sum(r[1] for r in runs)
+        rb = np.array([r[2] for r in runs])
+        wts = np.array([r[0] for r in runs], float)
+        mean = float(np.sum(rb * wts) / wts.sum())
+        # batch means, weighted by each call's photons
+        var = float(np.sum(wts * (rb - mean) ** 2) / wts.sum() / (len(rb) - 1))
+        jobs.append({"job": k, "mua": float(p.mua[1]), "photons_of_job": int(job.photons),
+                     "photons_run": fins, "calls": len(runs), "seconds": secs,
+                     "value": fins / secs, "unit": "photons/s", "r_total": mean,
+                     "r_total_sigma_batch_means": float(np.sqrt(var))})
         fin_all += fins
         sec_all += secs
         stratum_photons = sum(int(w.jobs[j].photons) for j in strata[s_idx])
@@ -527,12 +542,14 @@ def reference_sweep(args, exe: Path) -> dict:
             "subset": {"jobs": jobs, "photons": fin_all, "seconds": sec_all,
                        "value": fin_all / sec_all, "unit": "photons/s",
                        "how": f"one seeded job per mua stratum ({SWEEP_STRATA} strata of "
-                              f"{len(w.jobs) // SWEEP_STRATA}), full photon count, "
-                              f"{nb} run_3dmc_gpu calls per job, wall time of each call"},
+                              f"{len(w.jobs) // SWEEP_STRATA}); four run_3dmc_gpu calls per "
+                              "job (230,400 photons, then three sized to "
+                              f"{args.sweep_ref_seconds:.0f} s in all, at most the job's "
+                              "count); wall time of each call"},
             "full_sweep_estimate": {"seconds": t_est, "value": w.photons / t_est,
                                     "unit": "photons/s",
-                                    "how": "each stratum's photons x its drawn job's seconds "
-                                           "per finished photon"}}
+                                    "how": "each stratum's photons x its sampled job's "
+                                           "seconds per finished photon"}}
 
 
 def run_reference_batched(args, exe: Path):
@@ -606,8 +623,9 @@ def run_reference(args):
     secs, fins = [], []
     for k in range(args.warmup + args.steps):
         out = tmp / f"r{k}"
+        n = int(args.ref_warmup_photons) if k < args.warmup else int(args.ref_photons)
         subprocess.run([str(exe), str(tmp / "geom.bin"), str(tmp / "props.bid"),
-                        str(int(args.ref_photons)), str(1796308352 + k), str(out),
+                        str(n), str(1796308352 + k), str(out),
                         str(exe.parent)], check=True, stdout=subprocess.DEVNULL,
                        stderr=subprocess.DEVNULL)
         raw = (tmp / f"r{k}_ref.bin").read_bytes()
@@ -629,6 +647,7 @@ def run_reference(args):
                                             "that 20 steps end within minutes; the "
                                             "reference's fixed 230,400-slot drain tail "
                                             "weighs a little more at 1e7",
+                   "warmup": f"{int(args.ref_warmup_photons)} photons per warm-up call",
                    "voxels": list(g.shape), "voxel_mm": g.dx, "beam": "uniform",
                    "parallelism": "single GPU (the reference has no multi-GPU path)"},
         "impl": "reference",
