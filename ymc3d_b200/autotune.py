@@ -16,10 +16,12 @@ import time
 
 from . import HERE, Job, Plan, default_table
 
-# (threads per block, blocks per SM; 0 = as many as fit).  Each block holds 28 KB of
-# per-thread tally columns sized for 256 threads, so blocks below 128 threads run
-# out of shared memory before they fill an SM's 768 threads.
-CANDIDATES = ((256, 0), (128, 0))
+# (threads per block, blocks per SM; 0 = as many as fit).  The photon kernels are
+# built for 80 registers, so an SM holds 768 of their threads: 3 blocks of 256 or 6
+# of 128 fill it (24 warps); 2 of 256 or 4 of 128 hold 16 warps, fewer to hide
+# latency with.  Each block holds 28 KB of per-thread tally columns sized for 256 threads, so
+# blocks below 128 threads run out of shared memory before they fill an SM.
+CANDIDATES = ((256, 0), (128, 0), (256, 2), (128, 4))
 _CACHE_FILE = HERE / "_data" / "tuning.json"
 _cache: dict | None = None
 

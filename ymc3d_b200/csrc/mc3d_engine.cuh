@@ -69,6 +69,8 @@ struct FloatTable {
 
 struct MathExact : FloatTable {
     static constexpr bool kFast = false;
+    /* a product rounded on its own, never fused into a following add */
+    static __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
     static __device__ __forceinline__ float div(float a, float b) { return a / b; }
     /* a / b where the caller also holds r = 1/b: the exact policy divides */
     static __device__ __forceinline__ float div_r(float a, float b, float) { return a / b; }
@@ -91,6 +93,7 @@ struct MathExact : FloatTable {
  * operators and functions below map to the approximate hardware paths. */
 struct MathFast : FloatTable {
     static constexpr bool kFast = true;
+    static __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
     /* every denominator divided here is a direction cosine, a sum of products of
      * cosines and sines, a refractive-index sum or 1 - g + 2 g xi, all far below the
      * 2^126 where __fdividef stops being defined; x / 0 still gives +-inf or NaN */
@@ -123,6 +126,7 @@ struct MathFast : FloatTable {
 struct MathF64 {
     using real = double;
     static constexpr bool kFast = false;
+    static __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
     static __device__ __forceinline__ double div(double a, double b) { return a / b; }
     static __device__ __forceinline__ double div_r(double a, double b, double) { return a / b; }
     static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
@@ -191,11 +195,16 @@ template <class M, class R = typename M::real>
 static __device__ __forceinline__ int grid_coord(R x, R ux, float d_, float rd_)
 {
     const R d = d_, rd = rd_;
-    int i = (int)M::floor(M::div_r(x, d, rd));
-    i += (x == (R)(int)((unsigned)i + 1u) * d);
-    R bmin = (R)i * d;
-    i = ((x > bmin) || ((x == bmin) && (ux >= 0))) ? i : i - 1;
-    return i;
+    /* the index is carried as a float (exact for |i| < 2^24), which saves the
+     * int <-> float conversions of the two face products */
+    R fi = M::floor(M::div_r(x, d, rd));
+    const R f1 = fi + (R)1;
+    const R hi = f1 * d;
+    const bool up = (x == hi);
+    fi = up ? f1 : fi;
+    const R bmin = up ? hi : fi * d;
+    const bool stay = (x > bmin) || ((x == bmin) && (ux >= 0));
+    return (int)fi - (stay ? 0 : 1);
 }
 
 /* src/mc3d_gpu.cu:24-27 with the clamp addressing of the texture (:416-418).
@@ -221,24 +230,25 @@ static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, 
 }
 
 /* src/mc3d_gpu.cu:29-49.  With r > 0 the box is the cube of voxels within
- * Chebyshev distance r of (i, j, k) instead of the voxel itself; axes, if given,
- * receives the snapped axes (bit 0 x, 1 y, 2 z). */
+ * Chebyshev distance r of (i, j, k) instead of the voxel itself.  Each border is
+ * a rounded product, as the reference's separate multiply gives it: fused into
+ * the subtraction that follows (which the compiler may do where the snapped
+ * positions are unused), a photon lying exactly on a face would see its
+ * distance to that face as the product's rounding error instead of 0. */
 template <class M, class R = typename M::real>
 static __device__ __forceinline__ R intersection(const GeomDev &g, int i, int j, int k, R *x, R ux,
-                                                 R *y, R uy, R *z, R uz, int r = 0,
-                                                 int *axes = nullptr)
+                                                 R *y, R uy, R *z, R uz, int r = 0)
 {
-    R border_x = (R)((ux >= 0) ? (int)((unsigned)i + 1u + r) : i - r) * (R)g.dx;
+    R border_x = M::mul_rn((R)((ux >= 0) ? (int)((unsigned)i + 1u + r) : i - r), (R)g.dx);
     R t_x = M::div(border_x - *x, ux);
-    R border_y = (R)((uy >= 0) ? (int)((unsigned)j + 1u + r) : j - r) * (R)g.dy;
+    R border_y = M::mul_rn((R)((uy >= 0) ? (int)((unsigned)j + 1u + r) : j - r), (R)g.dy);
     R t_y = M::div(border_y - *y, uy);
-    R border_z = (R)((uz >= 0) ? (int)((unsigned)k + 1u + r) : k - r) * (R)g.dz;
+    R border_z = M::mul_rn((R)((uz >= 0) ? (int)((unsigned)k + 1u + r) : k - r), (R)g.dz);
     R t_z = M::div(border_z - *z, uz);
     R t = M::fmin(t_x, M::fmin(t_y, t_z));
     *x = (t == t_x) ? border_x : *x + ux * t;
     *y = (t == t_y) ? border_y : *y + uy * t;
     *z = (t == t_z) ? border_z : *z + uz * t;
-    if (axes) *axes = (int)(t == t_x) | ((int)(t == t_y) << 1) | ((int)(t == t_z) << 2);
     return t;
 }
 
@@ -281,14 +291,22 @@ struct Acc {
 /* One step of src/mc3d_gpu.cu:175-340 for a live photon.  Returns true when the
  * photon froze during this step; *db receives the step's boundary distance.
  *
- * JUMP (merged steps): p.tissue carries the voxel's safe distance r in bits 8-15,
- * and the step's box is the cube of voxels within Chebyshev distance r of the
- * photon's voxel, all of the photon's tissue.  Its faces are voxel faces, so a
- * step that reaches one ends exactly where the reference's step at that face
- * ends (snapped, next voxel by the face rule, Fresnel, mirror), while the face
- * crossings inside the cube, which in the reference only move the photon (no
- * Fresnel event, absorption or scattering; their four random numbers are drawn
- * and discarded), are merged into this one step. */
+ * JUMP (merged steps): p.tissue carries a box radius r in bits 8-15, and the
+ * step's box is the cube of voxels within Chebyshev distance r of the photon's
+ * voxel.  r is one less than the voxel's safe distance, so the box and a shell
+ * of one voxel around it hold only the photon's tissue and stay clear of the top
+ * and lateral faces: a step that reaches a box face crosses into a voxel of the
+ * same tissue, with no Fresnel event, no mirror and no air rule, exactly as the
+ * reference's step at that face would (snapped, next voxel by the face rule).
+ * The face crossings inside the box, which in the reference only move the
+ * photon (no absorption or scattering; their four random numbers are drawn and
+ * discarded), are merged into this one step.  Every reflection therefore
+ * happens in a one-voxel step (r = 0), where the reference's rule applies
+ * unchanged: a reflected photon keeps the voxel index it started the step with
+ * (src/mc3d_gpu.cu:334-339).  That rule can leave the index one voxel off when a
+ * coordinate that was not snapped rounded onto a face; the photon then takes
+ * zero-length steps until the quickfix at its chunk's end removes it, which is
+ * part of the weight the reference loses. */
 template <class M, bool AMAP, bool JUMP = false, class R = typename M::real>
 static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float4 *tab,
                                                    PhotonT<R> &p, uint64_t &rx, uint32_t ra,
@@ -306,9 +324,8 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     const R rmu_t = M::rmu_t(tt);
 
     R newx = p.x, newy = p.y, newz = p.z;
-    int axes = 0;
     R db = intersection<M>(g, p.i, p.j, p.k, &newx, p.ux, &newy, p.uy, &newz, p.uz,
-                               JUMP ? (p.tissue >> 8) : 0, JUMP ? &axes : nullptr);
+                               JUMP ? (p.tissue >> 8) : 0);
 
     bool hit = db * mu_t <= p.s;
     R ds = hit ? db * mu_t : p.s;
@@ -323,21 +340,10 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     int next_tissue = tissue_at<JUMP>(g, nexti, nextj, nextk, newz, p.uz);
     nt = M::n(tab + MC3D_TAB_STRIDE * (JUMP ? (next_tissue & 0xff) : next_tissue));
 
-    /* The voxel on the near side of the crossed face, which the reference's face
-     * logic compares with the next voxel: the photon's own voxel in a one-voxel
-     * step, the last voxel of the cube in a merged one. */
-    int bi = p.i, bj = p.j, bk = p.k;
-    if (JUMP) {
-        const int ax = hit ? axes : 0;
-        bi = nexti - ((ax & 1) ? ((p.ux >= 0) ? 1 : -1) : 0);
-        bj = nextj - ((ax & 2) ? ((p.uy >= 0) ? 1 : -1) : 0);
-        bk = nextk - ((ax & 4) ? ((p.uz >= 0) ? 1 : -1) : 0);
-    }
-
     R tr_ux = p.ux, tr_uy = p.uy, tr_uz = p.uz;
     bool refl = false;
     if (ni != nt) { /* src/mc3d_gpu.cu:226-257 */
-        R cos_ai = (bi != nexti) ? p.ux : ((bj != nextj) ? p.uy : p.uz);
+        R cos_ai = (p.i != nexti) ? p.ux : ((p.j != nextj) ? p.uy : p.uz);
         cos_ai = M::fabs(cos_ai);
         cos_ai = (cos_ai > 1) ? 1 : cos_ai;
         R ai = M::acos(cos_ai);
@@ -363,9 +369,9 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
             const double R1 = (si * ca - c * st) / (si * ca + c * st);
             const double R2 = (c * ca - si * st) / (c * ca + st * st);
             Rf = (st >= 1.0) ? (R)1 : (R)(0.5 * R1 * R1 * (1.0 + R2 * R2));
-            const bool xa = bi != nexti;
-            const bool ya = !xa && bj != nextj;
-            const bool za = !xa && !ya && bk != nextk;
+            const bool xa = p.i != nexti;
+            const bool ya = !xa && p.j != nextj;
+            const bool za = !xa && !ya && p.k != nextk;
             const double ax = xa ? 0.0 : (double)p.ux;
             const double ay = ya ? 0.0 : (double)p.uy;
             const double az = za ? 0.0 : (double)p.uz;
@@ -376,13 +382,13 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
         }
         float eps = mc3d_rand_co(&rx, ra);
         refl = eps < Rf;
-        tr_ux = refl ? p.ux * ((bi == nexti) ? 1 : -1)
-                     : ((bi != nexti) ? M::copysign(cos_at, p.ux * cos_at) : p.ux * lat);
-        tr_uy = refl ? p.uy * ((bj == nextj) ? 1 : -1)
-                     : (((bj != nextj) && (bi == nexti)) ? M::copysign(cos_at, p.uy * cos_at)
+        tr_ux = refl ? p.ux * ((p.i == nexti) ? 1 : -1)
+                     : ((p.i != nexti) ? M::copysign(cos_at, p.ux * cos_at) : p.ux * lat);
+        tr_uy = refl ? p.uy * ((p.j == nextj) ? 1 : -1)
+                     : (((p.j != nextj) && (p.i == nexti)) ? M::copysign(cos_at, p.uy * cos_at)
                                                            : p.uy * lat);
-        tr_uz = refl ? p.uz * ((bk == nextk) ? 1 : -1)
-                     : (((bk != nextk) && (bj == nextj) && (bi == nexti))
+        tr_uz = refl ? p.uz * ((p.k == nextk) ? 1 : -1)
+                     : (((p.k != nextk) && (p.j == nextj) && (p.i == nexti))
                             ? M::copysign(cos_at, p.uz * cos_at)
                             : p.uz * lat);
         (*fresnel_count)++;
@@ -475,21 +481,10 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
     *lat_mirror = refl && !fres_refl;
 
     bool keep = (hit && refl) || freeze;
-    if (JUMP) {
-        /* a reflected photon stays on the near side of the face: that voxel has
-         * the photon's tissue; its safe distance is not at hand, so 0 (one
-         * per-face step) until the photon moves on */
-        const bool back = hit && refl && !freeze;
-        p.i = freeze ? p.i : (back ? bi : nexti);
-        p.j = freeze ? p.j : (back ? bj : nextj);
-        p.k = freeze ? p.k : (back ? bk : nextk);
-        p.tissue = freeze ? p.tissue : (back ? (p.tissue & 0xff) : next_tissue);
-    } else {
-        p.i = keep ? p.i : nexti;
-        p.j = keep ? p.j : nextj;
-        p.k = keep ? p.k : nextk;
-        p.tissue = keep ? p.tissue : next_tissue;
-    }
+    p.i = keep ? p.i : nexti;
+    p.j = keep ? p.j : nextj;
+    p.k = keep ? p.k : nextk;
+    p.tissue = keep ? p.tissue : next_tissue;
     *db_out = db;
     return freeze;
 }

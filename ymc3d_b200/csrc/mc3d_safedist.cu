@@ -97,6 +97,9 @@ __global__ void pass_minmax_kernel(const uint8_t *__restrict__ in, int nx, int n
     }
 }
 
+/* the merged kernel's cells: tissue | box radius << 8, the radius one less than the
+ * safe distance, so that a box face never coincides with a tissue boundary or a
+ * top or lateral face (every reflection then happens in a one-voxel step) */
 __global__ void pack_kernel(const uint8_t *__restrict__ t, const uint8_t *__restrict__ r, int nx,
                             int ny, int nz, int nz_map, uint16_t *__restrict__ out)
 {
@@ -105,7 +108,8 @@ __global__ void pack_kernel(const uint8_t *__restrict__ t, const uint8_t *__rest
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
          v += (int64_t)gridDim.x * blockDim.x) {
         const int k = (int)(v / plane);
-        out[v] = (uint16_t)(t[(int64_t)min(k, nz - 1) * plane + v % plane] | ((int)r[v] << 8));
+        const int box = max((int)r[v] - 1, 0);
+        out[v] = (uint16_t)(t[(int64_t)min(k, nz - 1) * plane + v % plane] | (box << 8));
     }
 }
 
