@@ -19,8 +19,9 @@ from . import HERE, Job, Plan, default_table
 # (threads per block, blocks per SM; 0 = as many as fit).  The photon kernels are
 # built for 80 registers, so an SM holds 768 of their threads: 3 blocks of 256 or 6
 # of 128 fill it (24 warps); 2 of 256 or 4 of 128 hold 16 warps, fewer to hide
-# latency with.  Each block holds 28 KB of per-thread tally columns sized for 256 threads, so
-# blocks below 128 threads run out of shared memory before they fill an SM.
+# latency with.  Each block holds 28 KB of per-thread tally columns sized for 256
+# threads, so blocks below 128 threads run out of shared memory before they fill
+# an SM.
 CANDIDATES = ((256, 0), (128, 0), (256, 2), (128, 4))
 _CACHE_FILE = HERE / "_data" / "tuning.json"
 _cache: dict | None = None
@@ -83,8 +84,10 @@ def tune(geoms, props, jobs, table=None, math: str = "fast", device: int = 0,
     table = default_table() if table is None else table
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     if not sample_streams:
-        # two streams per thread of a full-occupancy grid, shared by the jobs
-        sample_streams = max(1, (sms * 1024 * 2) // max(1, len(jobs)))
+        # sixteen streams per thread of a full grid (768 threads per SM), shared by the
+        # jobs: a launch's tail is about one photon per thread, and it favours fewer
+        # threads, so a short sample would pick shapes that lose in the steady state
+        sample_streams = max(1, (sms * 768 * 16) // max(1, len(jobs)))
     sample = _sample_jobs(jobs, sample_streams)
     stream = torch.cuda.Stream(device)
     results = []
