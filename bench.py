@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--photons", type=float, default=1e8, help="photons per GPU per job")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--math", default="fast", choices=["fast", "exact", "f64"])
     ap.add_argument("--ref-photons", type=float, default=1e7)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -301,6 +301,7 @@ def run_ours(args):
             te = float(tt.item())
         e2e = {"value": e2e_photons / len(e2e_times) / te, "unit": "photons/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": te * 1e3,
+               "samples_ms": [round(t * 1e3, 1) for t in e2e_times],
                "warmup": "one untimed mc3d_run of the warm-up job",
                "timing": "host clock around the synchronous mc3d_run call (plan, upload, "
                          "kernel, read-back), max over ranks"}

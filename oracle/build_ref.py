@@ -24,7 +24,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF = Path(os.environ.get("YMC3D_REFERENCE", "/root/reference"))
+# the reference checkout: $YMC3D_REFERENCE, else a directory named `reference`
+# beside this repository
+REF = Path(os.environ.get("YMC3D_REFERENCE", HERE.parent.parent / "reference"))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 TABLE_LINES = 1 + 230400  # n_rng = 600 blocks * 384 threads (src/mc3d_gpu.cu:434)
 
