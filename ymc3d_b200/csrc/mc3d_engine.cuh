@@ -346,9 +346,11 @@ static __device__ __forceinline__ bool photon_step(const GeomDev &g, const float
         R cos_ai = (p.i != nexti) ? p.ux : ((p.j != nextj) ? p.uy : p.uz);
         cos_ai = M::fabs(cos_ai);
         cos_ai = (cos_ai > 1) ? 1 : cos_ai;
-        R ai = M::acos(cos_ai);
         R ni_nt = M::div(ni, nt);
-        R sin_ai = M::sin(ai);
+        /* sin(acos(c)); fast math evaluates it as sqrt((1 - c)(1 + c)), the same
+         * value without the polynomial of acosf (and more accurate near c = 1) */
+        R sin_ai = M::kFast ? M::sqrt(((R)1 - cos_ai) * ((R)1 + cos_ai))
+                            : M::sin(M::acos(cos_ai));
         R sin_at = ni_nt * sin_ai;
         R cos_at = M::sqrt((R)1 - sin_at * sin_at);
         R R1 = M::div(sin_ai * cos_at - cos_ai * sin_at, sin_ai * cos_at + cos_ai * sin_at);
