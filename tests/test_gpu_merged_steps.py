@@ -136,3 +136,33 @@ def test_merged_quickfix_loss_matches_voxel_steps(table):
     for key in ("r_in", "r_out", "absorbed"):
         assert abs(total_z(mer.totals, vox.totals, key)) < 5, key
     assert residual(mer.totals) == 0 and residual(vox.totals) == 0
+
+
+def test_merged_vs_voxel_many_interfaces(table):
+    """Blocks of four tissues with different refractive indices and in-volume air:
+    most reflections (Fresnel, lateral mirror, total internal reflection at the
+    air) happen next to a tissue boundary, where merged steps shrink to one-voxel
+    steps.  Both step modes must give the same DRS, totals and quickfix losses."""
+    rng = np.random.default_rng(11)
+    coarse = rng.integers(1, 5, (6, 8, 8)).astype(np.uint8)
+    t = np.kron(coarse, np.ones((6, 6, 6), np.uint8))
+    t[rng.random(t.shape) < 0.002] = 0  # scattered in-volume air voxels
+    t[:3] = 1  # a uniform top layer
+    g = m.Geometry(t, 0.02, 0.02, 0.02)
+    p = m.OpticalProps.from_tissues([(0.05, 15.0, 0.85, 1.37), (0.2, 20.0, 0.9, 1.44),
+                                     (0.02, 10.0, 0.8, 1.50), (1.0, 25.0, 0.95, 1.33)])
+    n = 2_000_000
+    mer = m.run([g], [p], [m.Job(0, 0, n, 71, "uniform")], table=table)[0]
+    vox = m.run([g], [p], [m.Job(0, 0, n, 72, "uniform")], table=table, steps="voxel")[0]
+    chi2, dof, pv = drs_chi2(mer.drs, mer.drs_sq, mer.photons, vox.drs, vox.drs_sq, vox.photons,
+                             f=4)
+    assert dof > 100 and pv > 1e-4, (chi2, dof, pv)
+    for key in ("r_in", "r_out", "t_in", "absorbed"):
+        assert abs(total_z(mer.totals, vox.totals, key)) < 5, key
+    assert mer.totals["fresnel"] > 0 and mer.totals["t_in"] > 0
+    qm, qv = mer.totals["quickfix"], vox.totals["quickfix"]
+    assert abs(qm - qv) < 4 * np.sqrt(qm + qv + 1), (qm, qv)
+    # Fresnel events per photon agree too: every one is a one-voxel step
+    fm, fv = mer.totals["fresnel"], vox.totals["fresnel"]
+    assert abs(fm - fv) < 0.02 * fv, (fm, fv)
+    assert residual(mer.totals) == 0 and mer.totals["steps"] < vox.totals["steps"]

@@ -112,3 +112,23 @@ def test_long_path_medium_vs_reference(tmp_path, table):
         var = r.drs_sq.sum() / m.WEIGHT_SCALE / r.photons - total ** 2
         sigma = np.sqrt(var * (1 / fin + 1 / r.photons))
         assert abs(total - total_ref) < 4 * sigma, (steps, total, total_ref, sigma)
+
+
+def test_ellipsoid_inclusions_vs_reference(tmp_path, table):
+    """A geometry of the uneven batch (ellipsoid inclusions of up to 8 tissues with
+    refractive indices 1.33-1.50): curved interfaces, where the merged boxes
+    shrink and Fresnel events happen at every angle."""
+    from ymc3d_b200.workloads import uneven
+    w = uneven(ngeoms=1, photons=1, max_dim=96, rng_seed=4)
+    g, p = w.geoms[0], w.props[0]
+    rows = np.stack([p.mua, p.mus, p.g, p.n], 1)[1:]
+    R, fin = run_reference(tmp_path, g, rows, 1_000_000, 424243)
+    r = m.run([g], [p], [m.Job(0, 0, 4_000_000, 8080, "uniform")], table=table)[0]
+    chi2, dof, pv = compare(r, R, fin, 8)
+    assert dof >= 32 and pv > 1e-4, (chi2, dof, pv)
+    total_ref = R.sum() / fin
+    total = r.drs.sum() / m.WEIGHT_SCALE / r.photons
+    var = r.drs_sq.sum() / m.WEIGHT_SCALE / r.photons - total ** 2
+    sigma = np.sqrt(var * (1 / fin + 1 / r.photons))
+    assert abs(total - total_ref) < 4 * sigma, (total, total_ref, sigma)
+    assert r.totals["fresnel"] > r.photons  # interfaces are crossed
