@@ -44,10 +44,10 @@ OPS_JUMP = 8
 OPS_FRESNEL, SFU_FRESNEL = 37, 6
 FP32_LANES_PER_SM, SFU_LANES_PER_SM = 128, 16
 # DRAM bytes read + written by one photon-kernel launch of the layered workload
-# (ncu dram__bytes_read.sum + dram__bytes_write.sum = 30,415,104 + 3,840 on a
+# (ncu dram__bytes_read.sum + dram__bytes_write.sum = 30,852,096 + 0 on a
 # 1e7-photon launch): the first touch of grid, packed cell map, table and tallies,
 # independent of the photon count
-TRAFFIC_BYTES_PER_LAUNCH = 30_418_944
+TRAFFIC_BYTES_PER_LAUNCH = 30_852_096
 
 
 def parse():
