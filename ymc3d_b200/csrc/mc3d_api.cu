@@ -120,6 +120,33 @@ int list_rejections(const mc3d_seed_consts &sc, uint64_t seed, const uint32_t *t
     return MC3D_OK;
 }
 
+/* Refractive-index classes of geometry `gi`'s tissues 0..max_tissue: two tissues
+ * share a class when their index is equal in every optical set that a job uses
+ * with this geometry; air (tissue 0) has a class of its own.  Returns whether two
+ * tissues share one (otherwise the class map equals the tissue map). */
+bool index_classes(int gi, int max_tissue, const mc3d_props *props, const mc3d_job *jobs,
+                   int njobs, uint8_t classes[256])
+{
+    std::vector<int> sets;
+    for (int j = 0; j < njobs; j++)
+        if (jobs[j].geom == gi && std::find(sets.begin(), sets.end(), jobs[j].props) == sets.end())
+            sets.push_back(jobs[j].props);
+    for (int t = 0; t < 256; t++) classes[t] = (uint8_t)t;
+    if (sets.empty()) return false;
+    std::vector<std::vector<float>> keys; /* index of class c + 1 in each set */
+    bool shared = false;
+    for (int t = 1; t <= max_tissue; t++) {
+        std::vector<float> key;
+        for (int q : sets) key.push_back(props[q].n[t]);
+        size_t c = 0;
+        while (c < keys.size() && keys[c] != key) c++;
+        if (c == keys.size()) keys.push_back(key);
+        else shared = true;
+        classes[t] = (uint8_t)(c + 1);
+    }
+    return shared;
+}
+
 } /* namespace */
 
 /* the seeding helpers and the error text, for the other host files of the library */
@@ -391,21 +418,35 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         d.tissue = p->d_grids[i];
     }
     if (p->jump) {
-        /* per geometry: the safe-distance map into scratch, then packed with the
-         * tissue into 16-bit cells (scratch: two pass buffers and the map) */
+        /* per geometry: the safe-distance maps of the tissue grid and of its
+         * refractive-index classes, packed with the tissue into 16-bit cells
+         * (scratch: two pass buffers, the two maps and the class grid) */
         p->d_cells.assign(ngeoms, nullptr);
+        size_t max_vox = 0;
+        for (int i = 0; i < ngeoms; i++)
+            max_vox = std::max(max_vox, (size_t)geoms[i].nx * geoms[i].ny * geoms[i].nz);
         uint8_t *tmp = nullptr;
-        PLAN_TRY(cudaMalloc(&tmp, 3 * max_map));
+        PLAN_TRY(cudaMalloc(&tmp, 4 * max_map + max_vox));
+        uint8_t *map_t = tmp + 2 * max_map, *map_n = tmp + 3 * max_map, *cls = tmp + 4 * max_map;
         cudaError_t e = cudaSuccess;
         for (int i = 0; i < ngeoms && e == cudaSuccess; i++) {
-            size_t nmap = (size_t)geoms[i].nx * geoms[i].ny * (geoms[i].nz + MC3D_SAFE_CAP);
+            const mc3d_geom &g = geoms[i];
+            size_t nmap = (size_t)g.nx * g.ny * (g.nz + MC3D_SAFE_CAP);
+            uint8_t classes[256];
+            const bool shared = index_classes(i, max_tissue[i], props, jobs, njobs, classes);
             e = cudaMalloc(&p->d_cells[i], 2 * nmap);
             if (e == cudaSuccess)
-                e = launch_safe_distance(p->d_grids[i], geoms[i].nx, geoms[i].ny, geoms[i].nz,
-                                         tmp + 2 * max_map, tmp, tmp + max_map, p->stream);
+                e = launch_safe_distance(p->d_grids[i], g.nx, g.ny, g.nz, map_t, tmp,
+                                         tmp + max_map, p->stream);
+            if (e == cudaSuccess && shared)
+                e = launch_index_classes(p->d_grids[i], (int64_t)g.nx * g.ny * g.nz, classes, cls,
+                                         p->stream);
+            if (e == cudaSuccess && shared)
+                e = launch_safe_distance(cls, g.nx, g.ny, g.nz, map_n, tmp, tmp + max_map,
+                                         p->stream);
             if (e == cudaSuccess)
-                e = launch_pack_cells(p->d_grids[i], tmp + 2 * max_map, geoms[i].nx, geoms[i].ny,
-                                      geoms[i].nz, p->d_cells[i], p->stream);
+                e = launch_pack_cells(p->d_grids[i], map_t, shared ? map_n : map_t, g.nx, g.ny,
+                                      g.nz, p->d_cells[i], p->stream);
             gh[i].cells = p->d_cells[i];
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);

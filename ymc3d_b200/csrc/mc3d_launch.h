@@ -45,8 +45,15 @@ cudaError_t launch_seed_dump(const KernelParams &P, int64_t first, int64_t count
  * nx * ny * (nz + MC3D_SAFE_CAP) bytes each */
 cudaError_t launch_safe_distance(const uint8_t *tissue, int nx, int ny, int nz, uint8_t *out,
                                  uint8_t *tmp_a, uint8_t *tmp_b, cudaStream_t stream);
-cudaError_t launch_pack_cells(const uint8_t *tissue, const uint8_t *radius, int nx, int ny, int nz,
-                              uint16_t *cells, cudaStream_t stream);
+/* packed cells (tissue | box radius << 8) from the safe distances of the tissue grid
+ * (radius) and of its refractive-index classes (radius_n; the same map when every
+ * tissue has its own class) */
+cudaError_t launch_pack_cells(const uint8_t *tissue, const uint8_t *radius,
+                              const uint8_t *radius_n, int nx, int ny, int nz, uint16_t *cells,
+                              cudaStream_t stream);
+/* out[v] = classes[tissue[v]] for nv voxels (classes: 256 entries, host memory) */
+cudaError_t launch_index_classes(const uint8_t *tissue, int64_t nv, const uint8_t *classes,
+                                 uint8_t *out, cudaStream_t stream);
 cudaError_t launch_mwc_draws(const uint64_t *x, const uint32_t *a, int64_t ngen, int64_t n,
                              float *out, cudaStream_t stream);
 

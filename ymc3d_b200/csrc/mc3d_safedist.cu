@@ -97,20 +97,39 @@ __global__ void pass_minmax_kernel(const uint8_t *__restrict__ in, int nx, int n
     }
 }
 
-/* the merged kernel's cells: tissue | box radius << 8, the radius one less than the
- * safe distance, so that a box face never coincides with a tissue boundary or a
- * top or lateral face (every reflection then happens in a one-voxel step) */
-__global__ void pack_kernel(const uint8_t *__restrict__ t, const uint8_t *__restrict__ r, int nx,
-                            int ny, int nz, int nz_map, uint16_t *__restrict__ out)
+/* the merged kernel's cells: tissue | box radius << 8.  r is the safe distance of
+ * the tissue grid (the box holds one tissue); rn is the safe distance of the grid of
+ * refractive-index classes (tissues whose index is equal in every optical set used
+ * with the geometry share a class).  The box radius min(r, rn - 1) keeps a shell of
+ * one voxel between the box and any index change, top face or lateral face, so
+ * every reflection happens in a one-voxel step, while a box may still end at a
+ * boundary between tissues of equal index, where the reference's step only moves
+ * the photon on. */
+__global__ void pack_kernel(const uint8_t *__restrict__ t, const uint8_t *__restrict__ r,
+                            const uint8_t *__restrict__ rn, int nx, int ny, int nz, int nz_map,
+                            uint16_t *__restrict__ out)
 {
     const int64_t plane = (int64_t)nx * ny;
     const int64_t nv = plane * nz_map;
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
          v += (int64_t)gridDim.x * blockDim.x) {
         const int k = (int)(v / plane);
-        const int box = max((int)r[v] - 1, 0);
+        const int box = min((int)r[v], max((int)rn[v] - 1, 0));
         out[v] = (uint16_t)(t[(int64_t)min(k, nz - 1) * plane + v % plane] | (box << 8));
     }
+}
+
+/* each voxel's refractive-index class, from a 256-entry table */
+struct ClassTable {
+    uint8_t c[256];
+};
+
+__global__ void class_kernel(const uint8_t *__restrict__ t, int64_t nv,
+                             const __grid_constant__ ClassTable lut, uint8_t *__restrict__ out)
+{
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+         v += (int64_t)gridDim.x * blockDim.x)
+        out[v] = lut.c[t[v]];
 }
 
 int grid_for(int64_t nv)
@@ -135,13 +154,25 @@ cudaError_t launch_safe_distance(const uint8_t *tissue, int nx, int ny, int nz, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_pack_cells(const uint8_t *tissue, const uint8_t *radius, int nx, int ny, int nz,
-                              uint16_t *cells, cudaStream_t stream)
+cudaError_t launch_pack_cells(const uint8_t *tissue, const uint8_t *radius,
+                              const uint8_t *radius_n, int nx, int ny, int nz, uint16_t *cells,
+                              cudaStream_t stream)
 {
     const int nz_map = nz + MC3D_SAFE_CAP;
     const int64_t nv = (int64_t)nx * ny * nz_map;
     if (nx <= 0 || ny <= 0 || nz <= 0) return cudaSuccess;
-    pack_kernel<<<grid_for(nv), 256, 0, stream>>>(tissue, radius, nx, ny, nz, nz_map, cells);
+    pack_kernel<<<grid_for(nv), 256, 0, stream>>>(tissue, radius, radius_n, nx, ny, nz, nz_map,
+                                                  cells);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_index_classes(const uint8_t *tissue, int64_t nv, const uint8_t *classes,
+                                 uint8_t *out, cudaStream_t stream)
+{
+    if (nv <= 0) return cudaSuccess;
+    ClassTable lut;
+    for (int t = 0; t < 256; t++) lut.c[t] = classes[t];
+    class_kernel<<<grid_for(nv), 256, 0, stream>>>(tissue, nv, lut, out);
     return cudaGetLastError();
 }
 
