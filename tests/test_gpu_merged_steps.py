@@ -166,3 +166,41 @@ def test_merged_vs_voxel_many_interfaces(table):
     fm, fv = mer.totals["fresnel"], vox.totals["fresnel"]
     assert abs(fm - fv) < 0.02 * fv, (fm, fv)
     assert residual(mer.totals) == 0 and mer.totals["steps"] < vox.totals["steps"]
+
+
+def test_merged_boxes_cross_equal_index_boundaries(table):
+    """Blobs of three tissues with one refractive index and a fourth with another
+    (and in-volume air): merged boxes may end at the equal-index boundaries, where
+    the reference's step only moves the photon into the next tissue's
+    coefficients, but keep their one-voxel margin at the index change.  Merged and
+    per-face steps agree in DRS, totals, Fresnel events and quickfix losses, and
+    the equal-index boundaries cost fewer merged steps than distinct indices do."""
+    rng = np.random.default_rng(12)
+    t = np.kron(rng.integers(1, 5, (5, 6, 6)), np.ones((8, 8, 8), np.int64)).astype(np.uint8)
+    t[rng.random(t.shape) < 0.001] = 0
+    g = m.Geometry(t, 0.01, 0.01, 0.01)
+    same = [(0.001, 20.0, 0.9, 1.4), (0.0012, 18.0, 0.9, 1.4), (0.0009, 22.0, 0.9, 1.4),
+            (0.002, 20.0, 0.9, 1.33)]
+    p = m.OpticalProps.from_tissues(same)
+    n = 1_000_000
+    mer = m.run([g], [p], [m.Job(0, 0, n, 81, "uniform")], table=table)[0]
+    vox = m.run([g], [p], [m.Job(0, 0, n, 82, "uniform")], table=table, steps="voxel")[0]
+    chi2, dof, pv = drs_chi2(mer.drs, mer.drs_sq, mer.photons, vox.drs, vox.drs_sq, vox.photons,
+                             f=4)
+    assert dof > 100 and pv > 1e-4, (chi2, dof, pv)
+    for key in ("r_in", "r_out", "t_in", "absorbed"):
+        assert abs(total_z(mer.totals, vox.totals, key)) < 5, key
+    qm, qv = mer.totals["quickfix"], vox.totals["quickfix"]
+    assert abs(qm - qv) < 4 * np.sqrt(qm + qv + 1), (qm, qv)
+    fm, fv = mer.totals["fresnel"], vox.totals["fresnel"]
+    assert abs(fm - fv) < 4 * np.sqrt(fm + fv), (fm, fv)
+    assert residual(mer.totals) == 0
+    # with four distinct indices the same grid merges fewer of its per-face steps
+    distinct = m.OpticalProps.from_tissues([(a, b, c, 1.30 + 0.05 * k)
+                                            for k, (a, b, c, _) in enumerate(same)])
+    dj = m.Job(0, 0, 200_000, 83, "uniform")
+    dm = m.run([g], [distinct], [dj], table=table)[0]
+    dv = m.run([g], [distinct], [dj], table=table, steps="voxel")[0]
+    same_ratio = mer.totals["steps"] / vox.totals["steps"]
+    distinct_ratio = dm.totals["steps"] / dv.totals["steps"]
+    assert same_ratio < 0.95 * distinct_ratio, (same_ratio, distinct_ratio)
