@@ -27,7 +27,7 @@ struct GeomDev {
     float rdx, rdy, rdz;   /* 1 / voxel size (fast math only) */
     float pad2;
     const uint8_t *tissue; /* nz*ny*nx, x fastest; 0 = air */
-    const uint16_t *cells; /* tissue | safe distance << 8, nz + MC3D_SAFE_CAP slices (merged) */
+    const uint16_t *cells; /* tissue | box radius << 8, nz + MC3D_SAFE_CAP slices (merged) */
 };
 
 struct JobDev {

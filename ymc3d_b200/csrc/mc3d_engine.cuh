@@ -208,8 +208,8 @@ static __device__ __forceinline__ int grid_coord(R x, R ux, float d_, float rd_)
 }
 
 /* src/mc3d_gpu.cu:24-27 with the clamp addressing of the texture (:416-418).
- * With JUMP the lookup reads the packed map (tissue | safe distance << 8, one
- * 16-bit load), so the safe distance rides in bits 8-15 of the result (0 above
+ * With JUMP the lookup reads the packed map (tissue | box radius << 8, one
+ * 16-bit load), so the box radius rides in bits 8-15 of the result (0 above
  * the surface, where the tissue is air). */
 template <bool JUMP = false, class R = float>
 static __device__ __forceinline__ int tissue_at(const GeomDev &g, int i, int j, int k, R z, R uz)
