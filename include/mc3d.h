@@ -61,10 +61,10 @@ enum mc3d_math { MC3D_MATH_FAST = 0, MC3D_MATH_EXACT = 1, MC3D_MATH_F64 = 2 };
  * the reference does (src/mc3d_gpu.cu:181-339).  Both are the reference's
  * physics, including the weight its end-of-chunk quickfix removes
  * (src/mc3d_gpu.cu:343-353): a box holds one tissue and stops one voxel short of
- * any refractive-index change or top or lateral face, so every reflection happens
- * in a one-voxel step; only the step counts in mc3d_totals differ.  The mode applies to fast and
- * FP64 math; exact math always steps at every face, and so does a launch with a
- * geometry of nx * ny * (nz + 63) >= 2^32 voxels. */
+ * any refractive-index change or top or lateral face, so every reflection
+ * happens in a one-voxel step; only the step counts in mc3d_totals differ.  The
+ * mode applies to fast and FP64 math; exact math always steps at every face, and
+ * so does a launch with a geometry of nx * ny * (nz + 63) >= 2^32 voxels. */
 enum mc3d_steps { MC3D_STEPS_MERGED = 0, MC3D_STEPS_VOXEL = 1 };
 
 /* Voxel geometry (geometry_t, src/mc3d_types.h:38-43), tissue indices as uint8
