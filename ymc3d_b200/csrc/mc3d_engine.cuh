@@ -293,11 +293,13 @@ struct Acc {
  *
  * JUMP (merged steps): p.tissue carries a box radius r in bits 8-15, and the
  * step's box is the cube of voxels within Chebyshev distance r of the photon's
- * voxel.  r is one less than the voxel's safe distance, so the box and a shell
- * of one voxel around it hold only the photon's tissue and stay clear of the top
- * and lateral faces: a step that reaches a box face crosses into a voxel of the
- * same tissue, with no Fresnel event, no mirror and no air rule, exactly as the
- * reference's step at that face would (snapped, next voxel by the face rule).
+ * voxel.  The box holds only the photon's tissue, and a shell of one voxel around
+ * it has the photon's refractive index and stays clear of the top and lateral
+ * faces (pack_kernel): a step that reaches a box face crosses into a voxel of the
+ * same index, with no Fresnel event, no mirror and no air rule, exactly as the
+ * reference's step at that face would (snapped, next voxel by the face rule; that
+ * voxel may hold another tissue of the same index, whose coefficients the next
+ * step uses).
  * The face crossings inside the box, which in the reference only move the
  * photon (no absorption or scattering; their four random numbers are drawn and
  * discarded), are merged into this one step.  Every reflection therefore
