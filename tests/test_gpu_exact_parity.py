@@ -92,6 +92,35 @@ def test_batched_jobs(table):
     _compare([g1, g2], [p1, p2], jobs, table)
 
 
+def test_ragged_grids(table):
+    """a one-voxel grid (every photon on the lateral mirrors, the bottom voxel
+    continued below by the clamp addressing) and a one-voxel-high slab with three
+    different voxel sizes, in one launch"""
+    p = m.OpticalProps.from_tissues([(0.5, 10.0, 0.9, 1.4)])
+    g1 = m.Geometry(np.ones((1, 1, 1), np.uint8), 0.1, 0.1, 0.1)
+    g2 = m.Geometry(np.ones((5, 1, 7), np.uint8), 0.05, 0.2, 0.13)
+    r = _compare([g1, g2], [p], [m.Job(0, 0, 2000, 8080, "uniform"),
+                                 m.Job(1, 0, 2000, 9090, "pencil")], table)
+    assert r[0].totals["quickfix"] > 0 and r[0].totals["r_in"] > 0
+    for g, rr, beam in ((g1, r[0], "uniform"), (g2, r[1], "pencil")):
+        fast = m.run([g], [p], [m.Job(0, 0, 20000, 77, beam)], table=table)[0]
+        assert residual(fast.totals) == 0 and fast.totals["photons"] == 20000
+
+
+def test_many_tissue_types(table):
+    """250 tissue types with random refractive indices in random voxels: Fresnel at
+    almost every face, optical-table lines up to the largest tissue index"""
+    rng = np.random.default_rng(250)
+    rows = [(rng.uniform(0.05, 1.0), rng.uniform(5, 20), rng.uniform(0.7, 0.95),
+             rng.uniform(1.33, 1.5)) for _ in range(250)]
+    g = m.Geometry(rng.integers(1, 251, (9, 10, 12)).astype(np.uint8), 0.1, 0.1, 0.1)
+    p = m.OpticalProps.from_tissues(rows)
+    r = _compare([g], [p], [m.Job(0, 0, 3000, 2501, "uniform")], table)
+    assert r[0].totals["fresnel"] > 50 * r[0].totals["photons"]
+    fast = m.run([g], [p], [m.Job(0, 0, 20000, 2502, "uniform")], table=table)[0]
+    assert residual(fast.totals) == 0 and fast.totals["photons"] == 20000
+
+
 def test_absorption_map(table):
     """the per-voxel absorbed weight (the reference's disabled tally,
     src/mc3d_gpu.cu:265-272) matches the oracle voxel for voxel and sums exactly to
