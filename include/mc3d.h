@@ -170,7 +170,11 @@ int mc3d_run(const mc3d_geom *geoms, int32_t ngeoms, const mc3d_props *props, in
              const mc3d_options *opt, mc3d_out *out);
 
 /* Reusable plan: inputs uploaded once, then executed any number of times.
- * execute() is asynchronous on `stream` (a cudaStream_t, NULL = the plan's own). */
+ * execute() is asynchronous on `stream` (a cudaStream_t, NULL = the plan's own).
+ * Plans (and mc3d_run) take their device memory from a pool private to the
+ * library, one per device; destroy() waits for the device and returns the memory
+ * to that pool, which keeps up to 4 GiB of it for the next plan and hands the rest
+ * back to the driver. */
 typedef struct mc3d_plan mc3d_plan;
 int mc3d_plan_create(mc3d_plan **plan, const mc3d_geom *geoms, int32_t ngeoms,
                      const mc3d_props *props, int32_t nprops, const mc3d_job *jobs,

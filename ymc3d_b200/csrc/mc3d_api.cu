@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <ctime>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -46,6 +47,59 @@ int fail(int code, const char *fmt, ...)
         if (e_ != cudaSuccess)                                                               \
             return fail(MC3D_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));             \
     } while (0)
+
+/* Plans take their device memory from a pool private to the library, one per
+ * device, by stream-ordered allocation on the plan's stream.  The pool keeps up to
+ * kPoolKeep bytes of freed memory, so a caller that runs plan after plan (one
+ * mc3d_run per wavelength, say) reuses it instead of handing it back to the driver
+ * and having it mapped again; a cudaFree of one plan's buffers took anywhere from
+ * 2 to 260 ms.  Freed memory beyond kPoolKeep goes back at the next
+ * synchronisation. */
+const uint64_t kPoolKeep = 4ull << 30;
+const int kMaxDevices = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[kMaxDevices];
+
+cudaError_t pool_of(int device, cudaMemPool_t *out)
+{
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pools[device]) {
+        cudaMemPoolProps pp;
+        memset(&pp, 0, sizeof pp);
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.handleTypes = cudaMemHandleTypeNone;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&pool, &pp);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = kPoolKeep;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return e;
+        }
+        g_pools[device] = pool;
+    }
+    *out = g_pools[device];
+    return cudaSuccess;
+}
+
+/* `bytes` of device memory from the pool, ordered on stream s */
+template <class T>
+cudaError_t pool_alloc(T **ptr, size_t bytes, int device, cudaStream_t s)
+{
+    *ptr = nullptr;
+    if (bytes == 0) return cudaSuccess;
+    cudaMemPool_t pool;
+    cudaError_t e = pool_of(device, &pool);
+    if (e != cudaSuccess) return e;
+    void *v = nullptr;
+    e = cudaMallocFromPoolAsync(&v, bytes, pool, s);
+    if (e == cudaSuccess) *ptr = static_cast<T *>(v);
+    return e;
+}
 
 /* bytes of optical tables and geometry descriptors per launch (shared memory:
  * 227 KB per block, less 28 KB of tally columns) */
@@ -205,17 +259,20 @@ static void plan_free(mc3d_plan *p)
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(p->device);
-    if (p->stream) cudaStreamSynchronize(p->stream);
-    for (uint8_t *g : p->d_grids) cudaFree(g);
-    for (uint16_t *r : p->d_cells) cudaFree(r);
-    cudaFree(p->d_jobs);
-    cudaFree(p->d_geoms);
-    cudaFree(p->d_props);
-    cudaFree(p->d_mult);
-    cudaFree(p->d_rej);
-    cudaFree(p->d_tally);
-    cudaFree(p->d_amap);
-    cudaFree(p->d_log);
+    /* executes may be in flight on any stream: wait for the device, as cudaFree
+     * would, before the buffers go back to the pool */
+    cudaDeviceSynchronize();
+    if (p->stream) {
+        std::vector<void *> bufs(p->d_grids.begin(), p->d_grids.end());
+        bufs.insert(bufs.end(), p->d_cells.begin(), p->d_cells.end());
+        for (void *b : {(void *)p->d_jobs, (void *)p->d_geoms, (void *)p->d_props,
+                        (void *)p->d_mult, (void *)p->d_rej, (void *)p->d_tally,
+                        (void *)p->d_amap, (void *)p->d_log})
+            bufs.push_back(b);
+        for (void *b : bufs)
+            if (b) cudaFreeAsync(b, p->stream);
+        cudaStreamSynchronize(p->stream);
+    }
     if (p->cancel_registered) cudaHostUnregister((void *)p->h_cancel);
     if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
     if (p->graph) cudaGraphDestroy(p->graph);
@@ -406,7 +463,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         const mc3d_geom &g = geoms[i];
         size_t nv = (size_t)g.nx * g.ny * g.nz;
         max_map = std::max(max_map, (size_t)g.nx * g.ny * (g.nz + MC3D_SAFE_CAP));
-        PLAN_TRY(cudaMalloc(&p->d_grids[i], nv));
+        PLAN_TRY(pool_alloc(&p->d_grids[i], nv, p->device, p->stream));
         PLAN_TRY(cudaMemcpyAsync(p->d_grids[i], g.tissue, nv, cudaMemcpyHostToDevice, p->stream));
         GeomDev &d = gh[i];
         memset(&d, 0, sizeof d);
@@ -426,7 +483,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         for (int i = 0; i < ngeoms; i++)
             max_vox = std::max(max_vox, (size_t)geoms[i].nx * geoms[i].ny * geoms[i].nz);
         uint8_t *tmp = nullptr;
-        PLAN_TRY(cudaMalloc(&tmp, 4 * max_map + max_vox));
+        PLAN_TRY(pool_alloc(&tmp, 4 * max_map + max_vox, p->device, p->stream));
         uint8_t *map_t = tmp + 2 * max_map, *map_n = tmp + 3 * max_map, *cls = tmp + 4 * max_map;
         cudaError_t e = cudaSuccess;
         for (int i = 0; i < ngeoms && e == cudaSuccess; i++) {
@@ -434,7 +491,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
             size_t nmap = (size_t)g.nx * g.ny * (g.nz + MC3D_SAFE_CAP);
             uint8_t classes[256];
             const bool shared = index_classes(i, max_tissue[i], props, jobs, njobs, classes);
-            e = cudaMalloc(&p->d_cells[i], 2 * nmap);
+            e = pool_alloc(&p->d_cells[i], 2 * nmap, p->device, p->stream);
             if (e == cudaSuccess)
                 e = launch_safe_distance(p->d_grids[i], g.nx, g.ny, g.nz, map_t, tmp,
                                          tmp + max_map, p->stream);
@@ -450,10 +507,10 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
             gh[i].cells = p->d_cells[i];
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
-        cudaFree(tmp);
+        cudaFreeAsync(tmp, p->stream);
         PLAN_TRY(e);
     }
-    PLAN_TRY(cudaMalloc(&p->d_geoms, sizeof(GeomDev) * ngeoms));
+    PLAN_TRY(pool_alloc(&p->d_geoms, sizeof(GeomDev) * ngeoms, p->device, p->stream));
     PLAN_TRY(cudaMemcpyAsync(p->d_geoms, gh.data(), sizeof(GeomDev) * ngeoms,
                              cudaMemcpyHostToDevice, p->stream));
 
@@ -473,19 +530,20 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
             e[1] = make_float4(mut, frac, rmut, inv2g);
             e[2] = make_float4(1 - g2, 1 - g, twog, 1 + g2);
         }
-    PLAN_TRY(cudaMalloc(&p->d_props, sizeof(float4) * entries));
+    PLAN_TRY(pool_alloc(&p->d_props, sizeof(float4) * entries, p->device, p->stream));
     PLAN_TRY(cudaMemcpyAsync(p->d_props, tab.data(), sizeof(float4) * entries,
                              cudaMemcpyHostToDevice, p->stream));
-    PLAN_TRY(cudaMalloc(&p->d_mult, sizeof(uint32_t) * table_len));
+    PLAN_TRY(pool_alloc(&p->d_mult, sizeof(uint32_t) * table_len, p->device, p->stream));
     PLAN_TRY(cudaMemcpyAsync(p->d_mult, table, sizeof(uint32_t) * table_len,
                              cudaMemcpyHostToDevice, p->stream));
 
     /* ---- jobs, then the seeding scan for rejected attempts */
-    PLAN_TRY(cudaMalloc(&p->d_jobs, sizeof(JobDev) * njobs));
+    PLAN_TRY(pool_alloc(&p->d_jobs, sizeof(JobDev) * njobs, p->device, p->stream));
     PLAN_TRY(cudaMemcpyAsync(p->d_jobs, jh.data(), sizeof(JobDev) * njobs,
                              cudaMemcpyHostToDevice, p->stream));
     size_t tally_words = 3 * (size_t)p->total_bins + (size_t)njobs * MC3D_NUM_TOTALS + 1;
-    PLAN_TRY(cudaMalloc(&p->d_tally, tally_words * sizeof(unsigned long long)));
+    PLAN_TRY(pool_alloc(&p->d_tally, tally_words * sizeof(unsigned long long), p->device,
+                        p->stream));
     unsigned long long *first_reject = p->d_tally; /* scratch reuse before the first run */
     PLAN_TRY(cudaMemsetAsync(first_reject, 0xff, sizeof(unsigned long long) * njobs, p->stream));
     PLAN_TRY(launch_seed_scan(p->d_jobs, njobs, p->d_mult, table_len, sc, scan_base,
@@ -512,7 +570,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         jh[j].rej_count = (int32_t)(rej.size() - jh[j].rej_offset);
     }
     if (rej.empty()) rej.push_back(RejectionDev{INT64_MAX, 0});
-    PLAN_TRY(cudaMalloc(&p->d_rej, sizeof(RejectionDev) * rej.size()));
+    PLAN_TRY(pool_alloc(&p->d_rej, sizeof(RejectionDev) * rej.size(), p->device, p->stream));
     PLAN_TRY(cudaMemcpyAsync(p->d_rej, rej.data(), sizeof(RejectionDev) * rej.size(),
                              cudaMemcpyHostToDevice, p->stream));
     if (any_rej)
@@ -520,8 +578,12 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
                                  cudaMemcpyHostToDevice, p->stream));
 
     if (p->total_voxels)
-        PLAN_TRY(cudaMalloc(&p->d_amap, sizeof(unsigned long long) * p->total_voxels));
-    if (p->h_log) PLAN_TRY(cudaMalloc(&p->d_log, sizeof(PhotonRecord) * std::max<int64_t>(1, p->total_photons)));
+        PLAN_TRY(pool_alloc(&p->d_amap, sizeof(unsigned long long) * p->total_voxels, p->device,
+                            p->stream));
+    if (p->h_log)
+        PLAN_TRY(pool_alloc(&p->d_log,
+                            sizeof(PhotonRecord) * std::max<int64_t>(1, p->total_photons),
+                            p->device, p->stream));
     if (p->h_cancel) {
         PLAN_TRY(cudaHostRegister((void *)p->h_cancel, sizeof(int32_t), cudaHostRegisterMapped));
         p->cancel_registered = true;
