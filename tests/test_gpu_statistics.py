@@ -115,6 +115,30 @@ def test_plan_reexecute_identical(table):
     assert a.totals == b.totals and np.array_equal(a.drs, b.drs)
 
 
+def test_plan_memory_returns_to_the_pool(table):
+    """plans take device memory from the library's pool and give it back: after
+    the first plan, creating and destroying more (merged-step maps, absorption
+    map, graph capture, mc3d_run) leaves the device's free memory where it was,
+    and a plan built after many others still gives the same tallies"""
+    import torch
+    g, p = layered_small()
+    jobs = [m.Job(0, 0, 50_000, 9, "uniform")]
+    first = m.run([g], [p], jobs, table=table)[0]
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for k in range(12):
+        plan = m.Plan([g], [p], jobs, table=table, use_graph=(k % 2 == 1))
+        plan.execute()
+        plan.read()
+        plan.close()
+        m.run([g], [p], jobs, table=table, absorption_map=(k % 3 == 0))
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info(0)[0]
+    assert free1 >= free0 - (64 << 20), (free0, free1)
+    again = m.run([g], [p], jobs, table=table)[0]
+    assert again.totals == first.totals and np.array_equal(again.drs, first.drs)
+
+
 def test_plan_graph_replay_identical(table):
     """a plan captured into a CUDA graph replays to the same tallies"""
     g, p = layered_small()

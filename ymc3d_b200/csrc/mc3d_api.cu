@@ -591,8 +591,11 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
     }
 
     /* ---- launch shape: one resident wave, all SMs */
-    cudaDeviceProp prop;
-    PLAN_TRY(cudaGetDeviceProperties(&prop, p->device));
+    /* the two attributes needed, not the whole cudaDeviceProp (a slower query) */
+    int num_sms = 0, smem_optin = 0;
+    PLAN_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, p->device));
+    PLAN_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                    p->device));
     p->block = opt.block ? opt.block : 256;
     p->smem = sizeof(float4) * entries + sizeof(GeomDev) * ngeoms;
     /* The kernels' static shared memory (28 KB of per-thread tallies) counts
@@ -604,7 +607,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         PLAN_TRY(p->math == MC3D_MATH_FAST    ? attributes_photon_fast(&fa)
                  : p->math == MC3D_MATH_EXACT ? attributes_photon_exact(&fa)
                                               : attributes_photon_f64(&fa));
-        const size_t max_dyn = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;
+        const size_t max_dyn = (size_t)smem_optin - fa.sharedSizeBytes;
         if (p->smem > max_dyn) {
             plan_free(p);
             return fail(MC3D_ERR_CAPACITY, "optical tables and geometry descriptors need %zu B "
@@ -624,7 +627,7 @@ int mc3d_plan_create(mc3d_plan **plan_out, const mc3d_geom *geoms, int32_t ngeom
         return fail(MC3D_ERR_CAPACITY, "kernel does not fit an SM with block %d", opt.block);
     }
     if (opt.blocks_per_sm > 0) bps = std::min(bps, (int)opt.blocks_per_sm);
-    p->grid = prop.multiProcessorCount * bps;
+    p->grid = num_sms * bps;
 
     KernelParams &P = p->P;
     memset(&P, 0, sizeof P);
