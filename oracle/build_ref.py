@@ -10,6 +10,10 @@ copied.  Products (all git-ignored, they travel with the working tree):
                             src/mc3d_photons.cu, src/mc3d_io.cu) driven by
                             ref/ref_main.cu; mc3d_gpu.cu gets ref/texture_shim.h
                             force-included because CUDA 12 removed texture references
+  _ref/gpu-mc-bridge        the reference's own command line (src/mc3d_main.cu,
+                            src/mc3d_io.cu) with run_3dmc_gpu forwarded to this
+                            repository's libmc3d.so by ref/mc3d_b200_bridge.cu:
+                            the drop-in as a maintainer would build it
   _ref/safeprimes_base32.txt  the safe-prime table the reference reads from its
                             working directory (not distributed with the reference)
 Flags follow CMakeLists.txt:18 (-use_fast_math, -Xptxas -v) with sm_100a for
@@ -80,6 +84,19 @@ def build(table=None) -> bool:
         _run([_nvcc(), "-c", HERE / "ref" / "ref_main.cu", "-o", obj, *flags])
         objs.append(obj)
         _run([_nvcc(), *ARCH, "-Xcompiler", "-fopenmp", *objs, "-o", exe, "-lgomp"])
+    lib = HERE.parent / "ymc3d_b200" / "libmc3d.so"
+    bridge = OUT / "gpu-mc-bridge"
+    deps = [HERE / "ref" / "mc3d_b200_bridge.cu", lib, HERE.parent / "include" / "mc3d.h"]
+    if lib.exists() and (not bridge.exists() or
+                         any(d.stat().st_mtime > bridge.stat().st_mtime for d in deps)):
+        flags = ["-O3", *ARCH, *inc, "-I", HERE.parent / "include"]
+        objs = []
+        for path in (src / "mc3d_main.cu", src / "mc3d_io.cu", HERE / "ref" / "mc3d_b200_bridge.cu"):
+            obj = OUT / ("bridge_" + path.name + ".o")
+            _run([_nvcc(), "-c", path, "-o", obj, *flags])
+            objs.append(obj)
+        _run([_nvcc(), *ARCH, *objs, "-o", bridge, "-L", lib.parent, "-lmc3d",
+              "-Xlinker", "-rpath=$ORIGIN/../../ymc3d_b200"])
     tab = OUT / "safeprimes_base32.txt"
     if not tab.exists():
         if table is None:

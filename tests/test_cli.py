@@ -58,6 +58,36 @@ def test_cli_run_matches_library(engine, tmp_path, table):
 
 
 @pytest.mark.gpu
+def test_reference_command_line_on_the_library(engine, tmp_path, table):
+    """The drop-in as a maintainer builds it: the reference's own main and file I/O
+    (src/mc3d_main.cu, src/mc3d_io.cu) linked with the bridge that forwards
+    run_3dmc_gpu to libmc3d.so.  Its 30,000,000 photons (src/mc3d_main.cu:57) under
+    MC3D_SEED write _drs.bin and _simparam.dat byte for byte as gpu-mc does for the
+    same inputs, photons and seed."""
+    bridge = ROOT / "oracle" / "_ref" / "gpu-mc-bridge"
+    if not bridge.exists():
+        pytest.skip("the bridge is built only where the reference's sources were present")
+    from ymc3d_b200.workloads import LAYER_ROWS, layered_vessel_geometry
+    g = layered_vessel_geometry(40, 36, 20, 0.1)
+    write_geometry_file(tmp_path / "geom.bin", g.tissue, g.dx, g.dy, g.dz)
+    write_optprops_file(tmp_path / "props.bid", LAYER_ROWS)
+    engine.write_safeprimes(tmp_path / "safeprimes_base32.txt", table[:230401])
+    seed = 271828182
+    import os
+    ref = subprocess.run([str(bridge), "geom.bin", "props.bid", "dummy", "ref"], cwd=tmp_path,
+                         capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, MC3D_SEED=str(seed)))
+    assert ref.returncode == 0, ref.stderr
+    assert "Total diffuse reflectance is" in ref.stderr
+    (tmp_path / "p.txt").write_text(f"photons = 30000000\nseed = {seed}\n")
+    ours = run(["geom.bin", "props.bid", "p.txt", "ours"], tmp_path)
+    assert ours.returncode == 0, ours.stderr
+    for suffix in ("_drs.bin", "_simparam.dat"):
+        assert (tmp_path / ("ref" + suffix)).read_bytes() == (tmp_path / ("ours" + suffix)).read_bytes()
+    assert (tmp_path / "ref_simparam.dat").read_text() == "30000000 #num_photons\n"
+
+
+@pytest.mark.gpu
 def test_cli_absorption_and_transmission_maps(engine, tmp_path, table):
     write_geometry_file(tmp_path / "geom.bin", np.ones((12, 16, 20), np.uint8), 0.1, 0.1, 0.1)
     write_optprops_file(tmp_path / "props.bid", [(0.3, 10.0, 0.9, 1.4)])
