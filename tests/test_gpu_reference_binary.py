@@ -132,3 +132,29 @@ def test_ellipsoid_inclusions_vs_reference(tmp_path, table):
     sigma = np.sqrt(var * (1 / fin + 1 / r.photons))
     assert abs(total - total_ref) < 4 * sigma, (total, total_ref, sigma)
     assert r.totals["fresnel"] > r.photons  # interfaces are crossed
+
+
+@pytest.mark.parametrize("which", ["least_absorbing", "most_absorbing"])
+def test_sweep_extremes_vs_reference(tmp_path, table, which):
+    """The metric's own workload: the hyperspectral sweep's least and most
+    absorbing optical sets (mua 0.001 and 0.92 /mm) on its 64^3 geometry at
+    0.1 mm, the engine's merged steps against run_3dmc_gpu.  The least absorbing
+    set has the longest paths, where the reference runs slowest."""
+    from ymc3d_b200.workloads import sweep
+    w = sweep(photon_scale=1.0, beam="uniform")
+    mua = np.array([float(w.props[j.props].mua[1]) for j in w.jobs])
+    k = int(mua.argmin() if which == "least_absorbing" else mua.argmax())
+    p = w.props[w.jobs[k].props]
+    rows = [(float(p.mua[1]), float(p.mus[1]), float(p.g[1]), float(p.n[1]))]
+    g = w.geoms[0]
+    R, fin = run_reference(tmp_path, g, rows,
+                           200_000 if which == "least_absorbing" else 1_000_000, 90210 + k)
+    r = m.run([g], [m.OpticalProps.from_tissues(rows)],
+              [m.Job(0, 0, 4_000_000, 31415 + k, "uniform")], table=table)[0]
+    chi2, dof, pv = compare(r, R, fin, 4)
+    assert dof >= 32 and pv > 1e-4, (chi2, dof, pv)
+    total_ref = R.sum() / fin
+    total = r.drs.sum() / m.WEIGHT_SCALE / r.photons
+    var = r.drs_sq.sum() / m.WEIGHT_SCALE / r.photons - total ** 2
+    sigma = np.sqrt(var * (1 / fin + 1 / r.photons))
+    assert abs(total - total_ref) < 4 * sigma, (total, total_ref, sigma)
